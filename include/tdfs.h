@@ -1,0 +1,121 @@
+/*
+ * tdfs.h -- C ABI of the B200 subgraph-enumeration engine (libtdfs_b200.so).
+ *
+ * Drop-in for the hot path of lyuheng/tdfs: the reference has no library API;
+ * its seam is graph load -> pattern plan -> one kernel launch -> u64 sum
+ * (cu_test.cu:14-107).  Each entry point below names the reference code it
+ * replaces.  Plain C types only; handles are opaque and caller-owned.  Every
+ * function returns 0 on success or a TDFS_ERR_* code, with a message from
+ * tdfs_last_error() (thread-local).  Calls on one handle must come from one
+ * host thread at a time.
+ */
+#ifndef TDFS_B200_H
+#define TDFS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TDFS_MAX_PATTERN 7 /* src/config.h:11 PAT_SIZE */
+
+enum {
+  TDFS_OK = 0,
+  TDFS_ERR_IO = 1,        /* missing/unreadable file (src/graph.h:127-130 exits) */
+  TDFS_ERR_FORMAT = 2,    /* malformed graph or pattern file */
+  TDFS_ERR_PATTERN = 3,   /* pattern outside the supported class */
+  TDFS_ERR_CUDA = 4,      /* CUDA runtime failure */
+  TDFS_ERR_CAPACITY = 5,  /* a device buffer limit was exceeded */
+  TDFS_ERR_TIMEOUT = 6,   /* a bounded device wait ran out */
+  TDFS_ERR_ARG = 7,       /* invalid argument */
+  TDFS_ERR_ADMISSION = 8  /* serving: query rejected by the memory budget */
+};
+
+typedef struct tdfs_graph tdfs_graph; /* device-resident data graph */
+typedef struct tdfs_plan tdfs_plan;   /* compiled pattern plan */
+typedef struct tdfs_csr tdfs_csr;     /* host CSR (generators, file reader) */
+
+/* Launch knobs.  Zero means "choose automatically". */
+typedef struct {
+  int warps_per_block;  /* warps per CTA */
+  int blocks_per_sm;    /* resident CTAs per SM */
+  int chunk_cap;        /* candidate slots per DFS level (multiple of 32) */
+  int steal;            /* 1: intra-block work stealing + global split queue; 0: off; -1 auto */
+  int merge_window;     /* merge-window size in ints (0 auto, -1 = binary search only) */
+  int64_t edge_begin;   /* level-0 directed-edge range [edge_begin, edge_end) */
+  int64_t edge_end;     /*   (0, -1 = all edges) */
+  int edge_stride;      /* level-0 chunks are dealt round-robin over edge_stride */
+  int edge_phase;       /*   shards; this call takes chunks == edge_phase (mod) */
+  void *stream;         /* cudaStream_t; NULL = legacy default stream */
+} tdfs_options;
+
+const char *tdfs_last_error(void);
+int tdfs_version(void);
+void tdfs_options_default(tdfs_options *opt);
+
+/* ---- data graph: replaces GraphPreprocessor(prefix) + to_gpu()
+ *      (src/graph.h:26-50, read_bin_file src/graph.h:136-193) ---------------
+ * Reads <prefix>.meta.txt / .vertex.bin / .edge.bin (and .label.bin when
+ * labeled) and uploads the CSR to `device`.  Rows must be strictly increasing
+ * (the reference asserts no duplicates, src/graph.h:186-192). */
+int tdfs_graph_open(const char *prefix, int labeled, int device, tdfs_graph **out);
+/* Same from caller host buffers (copied; labels may be NULL when unlabeled). */
+int tdfs_graph_from_csr(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx,
+                        const int32_t *labels, int device, tdfs_graph **out);
+int tdfs_graph_info(const tdfs_graph *g, int64_t *n, int64_t *nedges, int32_t *max_degree,
+                    int *labeled, size_t *device_bytes);
+int tdfs_graph_free(tdfs_graph *g);
+
+/* ---- pattern plan: replaces PatternPreprocessor(gfile) + to_gpu()
+ *      (src/pattern.h:90-108) ------------------------------------------------
+ * Matching order = file order; symmetry conditions from the full
+ * automorphism group; reuse levels; labels.  labeled selects lb semantics. */
+int tdfs_plan_compile(const char *gpath, int labeled, tdfs_plan **out);
+int tdfs_plan_from_text(const char *text, int labeled, tdfs_plan **out);
+/* JSON with the plan fields the reference kernel reads (for known-answer
+ * tests against src/pattern.h).  Returns the needed size in *len. */
+int tdfs_plan_dump(const tdfs_plan *p, char *buf, size_t cap, size_t *len);
+int tdfs_plan_info(const tdfs_plan *p, int *k, int *labeled, int64_t *multiplicity);
+int tdfs_plan_free(tdfs_plan *p);
+
+/* ---- count: replaces the _parallel_match launch + host reduction
+ *      (cu_test.cu:81-105; kernel src/gpu_match.cu:951-1080) ----------------
+ * *count = the number ulb/lb print (unlabeled totals already x |Aut|).
+ * *kernel_ms (nullable) = device time of the match kernel(s), as the
+ * reference's cudaEvent pair measures it (cu_test.cu:81-97). */
+int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint64_t *count,
+               float *kernel_ms);
+
+/* ---- batched launch (no reference counterpart; the north-star batching) --
+ * All plans run in one persistent launch; counts[i] belongs to plans[i]. */
+int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
+                     const tdfs_options *opt, uint64_t *counts, float *kernel_ms);
+
+/* ---- host CSR: generators and file writer (graph_converter/ output format,
+ *      graph_converter/compactify.cpp:172-195, labelize.cpp:130-133) ------- */
+int tdfs_csr_read(const char *prefix, int labeled, tdfs_csr **out);
+int tdfs_csr_view(const tdfs_csr *c, int64_t *n, int64_t *nedges, const int64_t **rowptr,
+                  const int32_t **colidx, const int32_t **labels, int32_t *max_degree);
+int tdfs_csr_write(const tdfs_csr *c, const char *prefix); /* .label.bin too when labelled */
+int tdfs_csr_set_labels(tdfs_csr *c, int nlabels, uint64_t seed); /* uniform [0, nlabels) */
+int tdfs_csr_free(tdfs_csr *c);
+/* Erdos-Renyi G(n, p), p = avg_degree / (n - 1) */
+int tdfs_gen_er(int64_t n, double avg_degree, uint64_t seed, tdfs_csr **out);
+/* Chung-Lu power law: ~undirected_edges edges, exponent gamma, degree cap,
+ * relabelled in descending-degree order (graph_converter/relabel.cpp:27-35) */
+int tdfs_gen_chung_lu(int64_t n, int64_t undirected_edges, double gamma, int32_t max_degree,
+                      uint64_t seed, tdfs_csr **out);
+/* R-MAT: 2^scale vertices, edge_factor * 2^scale samples, deduplicated and
+ * symmetrised, self-loops dropped */
+int tdfs_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint64_t seed,
+                  tdfs_csr **out);
+/* random connected pattern in valid matching order (vertex i>0 has an earlier
+ * neighbour, vertex 2 is adjacent to vertex 1) written as .g text */
+int tdfs_gen_pattern(int k, double density, int nlabels, uint64_t seed, char *buf, size_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,275 @@
+"""tdfs_b200 -- B200-native subgraph enumeration (drop-in for lyuheng/tdfs).
+
+Python mirror of the reference's host interface over the C ABI of
+libtdfs_b200.so (include/tdfs.h):
+
+* ``GraphPreprocessor(prefix, labeled)`` -- reads the reference's binary CSR
+  files and keeps the graph resident on the GPU (src/graph.h:26-50).
+* ``PatternPreprocessor(gfile, labeled)`` -- compiles a ``.g`` pattern into a
+  plan table (src/pattern.h:90-108).
+* ``count(graph, pattern)`` -- one launch of the DFS kernel; returns the count
+  ``ulb``/``lb`` print (cu_test.cu:81-107).
+
+There is no CPU execution path: every count runs the sm_100a kernels, and the
+module raises ``TdfsError`` when the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libtdfs_b200.so")
+BIN_DIR = os.path.join(_HERE, "bin")
+
+ERR_NAMES = {1: "IO", 2: "FORMAT", 3: "PATTERN", 4: "CUDA", 5: "CAPACITY", 6: "TIMEOUT", 7: "ARG",
+             8: "ADMISSION"}
+
+# every symbol include/tdfs.h declares (checked by the CPU tests)
+EXPORTS = [
+    "tdfs_last_error", "tdfs_version", "tdfs_options_default",
+    "tdfs_graph_open", "tdfs_graph_from_csr", "tdfs_graph_info", "tdfs_graph_free",
+    "tdfs_plan_compile", "tdfs_plan_from_text", "tdfs_plan_dump", "tdfs_plan_info", "tdfs_plan_free",
+    "tdfs_count", "tdfs_count_batch",
+    "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
+    "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern",
+]
+
+
+class TdfsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"TDFS_ERR_{ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    """Launch knobs (tdfs_options)."""
+    _fields_ = [
+        ("warps_per_block", C.c_int),
+        ("blocks_per_sm", C.c_int),
+        ("chunk_cap", C.c_int),
+        ("steal", C.c_int),
+        ("merge_window", C.c_int),
+        ("edge_begin", C.c_int64),
+        ("edge_end", C.c_int64),
+        ("edge_stride", C.c_int),
+        ("edge_phase", C.c_int),
+        ("stream", C.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libtdfs_b200.so (fails loudly when it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise TdfsError(4, f"{LIB_PATH} not built; run `python -m tdfs_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, i64, i32, ci = C.c_void_p, C.c_int64, C.c_int32, C.c_int
+    pp = C.POINTER(C.c_void_p)
+    L.tdfs_last_error.restype = C.c_char_p
+    L.tdfs_options_default.argtypes = [C.POINTER(Options)]
+    L.tdfs_options_default.restype = None
+    L.tdfs_graph_open.argtypes = [C.c_char_p, ci, ci, pp]
+    L.tdfs_graph_from_csr.argtypes = [i64, i64, vp, vp, vp, ci, pp]
+    L.tdfs_graph_info.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(ci),
+                                  C.POINTER(C.c_size_t)]
+    L.tdfs_graph_free.argtypes = [vp]
+    L.tdfs_plan_compile.argtypes = [C.c_char_p, ci, pp]
+    L.tdfs_plan_from_text.argtypes = [C.c_char_p, ci, pp]
+    L.tdfs_plan_dump.argtypes = [vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+    L.tdfs_plan_info.argtypes = [vp, C.POINTER(ci), C.POINTER(ci), C.POINTER(i64)]
+    L.tdfs_plan_free.argtypes = [vp]
+    L.tdfs_count.argtypes = [vp, vp, C.POINTER(Options), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+    L.tdfs_count_batch.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_float)]
+    L.tdfs_csr_read.argtypes = [C.c_char_p, ci, pp]
+    L.tdfs_csr_view.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), pp, pp, pp, C.POINTER(i32)]
+    L.tdfs_csr_write.argtypes = [vp, C.c_char_p]
+    L.tdfs_csr_set_labels.argtypes = [vp, ci, C.c_uint64]
+    L.tdfs_csr_free.argtypes = [vp]
+    L.tdfs_gen_er.argtypes = [i64, C.c_double, C.c_uint64, pp]
+    L.tdfs_gen_chung_lu.argtypes = [i64, i64, C.c_double, i32, C.c_uint64, pp]
+    L.tdfs_gen_rmat.argtypes = [ci, ci, C.c_double, C.c_double, C.c_double, C.c_uint64, pp]
+    L.tdfs_gen_pattern.argtypes = [ci, C.c_double, ci, C.c_uint64, C.c_char_p, C.c_size_t]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc:
+        raise TdfsError(rc, lib().tdfs_last_error().decode())
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().tdfs_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+# --------------------------------------------------------------------------
+# host CSR graphs (generators and the reference file format)
+# --------------------------------------------------------------------------
+
+class HostCSR:
+    """Host CSR owned by the library; numpy views share its memory."""
+
+    def __init__(self, handle: C.c_void_p):
+        self._h = handle
+        n, e, md = C.c_int64(), C.c_int64(), C.c_int32()
+        rp, ci, lb = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        _check(lib().tdfs_csr_view(handle, C.byref(n), C.byref(e), C.byref(rp), C.byref(ci), C.byref(lb),
+                                   C.byref(md)))
+        self.n, self.nedges, self.max_degree = n.value, e.value, md.value
+        self.rowptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int64)), shape=(self.n + 1,))
+        self.colidx = (np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), shape=(self.nedges,))
+                       if self.nedges else np.zeros(0, np.int32))
+        self.labels = (np.ctypeslib.as_array(C.cast(lb, C.POINTER(C.c_int32)), shape=(self.n,))
+                       if lb.value else None)
+
+    def set_labels(self, nlabels: int, seed: int) -> "HostCSR":
+        _check(lib().tdfs_csr_set_labels(self._h, nlabels, seed))
+        self.__init__(self._h)
+        return self
+
+    def write(self, prefix: str):
+        _check(lib().tdfs_csr_write(self._h, prefix.encode()))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.tdfs_csr_free(self._h)
+            self._h = None
+
+
+def read_csr(prefix: str, labeled: bool = False) -> HostCSR:
+    h = C.c_void_p()
+    _check(lib().tdfs_csr_read(prefix.encode(), int(labeled), C.byref(h)))
+    return HostCSR(h)
+
+
+def gen_er(n: int, avg_degree: float, seed: int) -> HostCSR:
+    h = C.c_void_p()
+    _check(lib().tdfs_gen_er(n, avg_degree, seed, C.byref(h)))
+    return HostCSR(h)
+
+
+def gen_chung_lu(n: int, undirected_edges: int, gamma: float, max_degree: int, seed: int) -> HostCSR:
+    h = C.c_void_p()
+    _check(lib().tdfs_gen_chung_lu(n, undirected_edges, gamma, max_degree, seed, C.byref(h)))
+    return HostCSR(h)
+
+
+def gen_rmat(scale: int, edge_factor: int, a: float, b: float, c: float, seed: int) -> HostCSR:
+    h = C.c_void_p()
+    _check(lib().tdfs_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(h)))
+    return HostCSR(h)
+
+
+def gen_pattern(k: int, density: float, nlabels: int, seed: int) -> str:
+    buf = C.create_string_buffer(1024)
+    _check(lib().tdfs_gen_pattern(k, density, nlabels, seed, buf, len(buf)))
+    return buf.value.decode()
+
+
+# --------------------------------------------------------------------------
+# reference-shaped front ends
+# --------------------------------------------------------------------------
+
+class GraphPreprocessor:
+    """Device-resident data graph (src/graph.h:26-50)."""
+
+    def __init__(self, prefix: str | None = None, labeled: bool = False, device: int = 0, *,
+                 csr: HostCSR | None = None, rowptr=None, colidx=None, labels=None):
+        h = C.c_void_p()
+        if prefix is not None:
+            _check(lib().tdfs_graph_open(prefix.encode(), int(labeled), device, C.byref(h)))
+        else:
+            if csr is not None:
+                rowptr, colidx = csr.rowptr, csr.colidx
+                labels = csr.labels if labeled else None
+            rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+            colidx = np.ascontiguousarray(colidx, dtype=np.int32)
+            lab = None if (labels is None or not labeled) else np.ascontiguousarray(labels, dtype=np.int32)
+            _check(lib().tdfs_graph_from_csr(len(rowptr) - 1, len(colidx), rowptr.ctypes.data,
+                                             colidx.ctypes.data, None if lab is None else lab.ctypes.data,
+                                             device, C.byref(h)))
+        self._h = h
+        n, e, md, lb, by = C.c_int64(), C.c_int64(), C.c_int32(), C.c_int(), C.c_size_t()
+        _check(lib().tdfs_graph_info(h, C.byref(n), C.byref(e), C.byref(md), C.byref(lb), C.byref(by)))
+        self.n, self.nedges, self.max_degree = n.value, e.value, md.value
+        self.labeled, self.device_bytes = bool(lb.value), by.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tdfs_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+class PatternPreprocessor:
+    """Compiled pattern plan (src/pattern.h:90-108)."""
+
+    def __init__(self, gfile: str | None = None, labeled: bool = False, *, text: str | None = None):
+        h = C.c_void_p()
+        if text is not None:
+            _check(lib().tdfs_plan_from_text(text.encode(), int(labeled), C.byref(h)))
+        else:
+            _check(lib().tdfs_plan_compile(gfile.encode(), int(labeled), C.byref(h)))
+        self._h = h
+        k, lb, m = C.c_int(), C.c_int(), C.c_int64()
+        _check(lib().tdfs_plan_info(h, C.byref(k), C.byref(lb), C.byref(m)))
+        self.nnodes, self.labeled, self.PatternMultiplicity = k.value, bool(lb.value), m.value
+
+    def dump(self) -> dict:
+        import json
+        n = C.c_size_t()
+        _check(lib().tdfs_plan_dump(self._h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(lib().tdfs_plan_dump(self._h, buf, n.value, None))
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().tdfs_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+
+@dataclass
+class CountResult:
+    count: int
+    kernel_ms: float
+
+
+def count(graph: GraphPreprocessor, pattern: PatternPreprocessor, options: Options | None = None) -> CountResult:
+    """Count embeddings as ulb/lb would print them."""
+    c = C.c_uint64()
+    ms = C.c_float()
+    _check(lib().tdfs_count(graph._h, pattern._h, None if options is None else C.byref(options), C.byref(c),
+                            C.byref(ms)))
+    return CountResult(c.value, ms.value)
+
+
+def count_batch(graph: GraphPreprocessor, patterns, options: Options | None = None):
+    """Counts for many patterns; returns (list of counts, kernel ms)."""
+    arr = (C.c_void_p * len(patterns))(*[p._h.value for p in patterns])
+    out = (C.c_uint64 * len(patterns))()
+    ms = C.c_float()
+    _check(lib().tdfs_count_batch(graph._h, arr, len(patterns), None if options is None else C.byref(options),
+                                  out, C.byref(ms)))
+    return list(out), ms.value

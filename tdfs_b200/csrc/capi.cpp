@@ -1,0 +1,266 @@
+// capi.cpp -- the extern "C" entry points of libtdfs_b200.so (include/tdfs.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "csr.h"
+#include "graph.h"
+#include "match.cuh"
+#include "plan.h"
+
+struct tdfs_plan {
+  tdfs::HostPlan host;
+  tdfs::DevPlan dev;
+};
+
+namespace tdfs {
+
+namespace {
+thread_local std::string g_error;
+}
+
+void set_error(const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_error = buf;
+}
+
+int fail(int code, const char *fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_error = buf;
+  return code;
+}
+
+namespace {
+
+struct LaunchShape {
+  int warps_per_block;
+  int blocks;
+  KernelCfg cfg;
+};
+
+int cuda_err(cudaError_t e, const char *what) {
+  return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Choose the launch shape: a persistent grid of (resident CTAs per SM) x SMs.
+int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, LaunchShape *out) {
+  cudaDeviceProp prop;
+  cudaError_t e = cudaGetDeviceProperties(&prop, g->device);
+  if (e != cudaSuccess) return cuda_err(e, "cudaGetDeviceProperties");
+  LaunchShape s;
+  std::memset(&s, 0, sizeof s);
+  s.warps_per_block = o.warps_per_block > 0 ? o.warps_per_block : 8;
+  if (s.warps_per_block > 8) return fail(TDFS_ERR_ARG, "warps_per_block must be <= 8");
+  int cap = o.chunk_cap > 0 ? o.chunk_cap : (p.k >= 6 ? 256 : 512);
+  cap = (cap + 31) & ~31;
+  if (cap < 64 || cap > 8192) return fail(TDFS_ERR_ARG, "chunk_cap must lie in [64, 8192]");
+  int window = o.merge_window == 0 ? 128 : (o.merge_window < 0 ? 0 : o.merge_window);
+  if (window % 128 != 0 || window > 256) return fail(TDFS_ERR_ARG, "merge_window must be 0, -1, 128 or 256");
+  KernelCfg &c = s.cfg;
+  c.cap = cap;
+  c.window = window;
+  c.warp_bytes = (int)((warp_smem_bytes(p.k, cap, window) + 15) & ~(size_t)15);
+  c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
+  c.poll_limit = 4096;
+  c.e_begin = std::max<int64_t>(0, o.edge_begin);
+  c.e_end = (o.edge_end < 0 || o.edge_end > g->nedges) ? g->nedges : o.edge_end;
+  c.stride = o.edge_stride > 0 ? o.edge_stride : 1;
+  c.phase = o.edge_phase;
+  if (c.phase < 0 || c.phase >= c.stride) return fail(TDFS_ERR_ARG, "edge_phase must lie in [0, edge_stride)");
+  const size_t smem = (size_t)c.warp_bytes * s.warps_per_block;
+  if (smem > (size_t)prop.sharedMemPerBlockOptin)
+    return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
+                smem, (size_t)prop.sharedMemPerBlockOptin);
+  int per_sm = o.blocks_per_sm;
+  if (per_sm <= 0) {
+    per_sm = (int)(prop.sharedMemPerMultiprocessor / (smem + prop.reservedSharedMemPerBlock));
+    per_sm = std::max(1, std::min(per_sm, prop.maxThreadsPerMultiProcessor / (32 * s.warps_per_block)));
+  }
+  s.blocks = prop.multiProcessorCount * per_sm;
+  *out = s;
+  return TDFS_OK;
+}
+
+// Launch the counting kernel for one plan on the graph's workspace and
+// return the raw (pre-multiplier) count.
+int run_one(tdfs_graph *g, const DevPlan &p, const tdfs_options &o, unsigned long long *raw, float *ms) {
+  if (p.labeled && !g->labeled) return fail(TDFS_ERR_ARG, "labeled pattern on a graph opened without labels");
+  cudaError_t e = cudaSetDevice(g->device);
+  if (e != cudaSuccess) return cuda_err(e, "cudaSetDevice");
+  LaunchShape s;
+  int rc = plan_launch(g, p, o, &s);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(o.stream);
+  QueueHdr *qh = queue_hdr(g);
+  const int total_warps = s.blocks * s.warps_per_block;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (ms) {
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+  }
+  init_launch(g->ctl, qh, total_warps, s.cfg.e_begin, st);
+  if (ms) cudaEventRecord(ev0, st);
+  rc = launch_match(p, graph_view(g), g->ctl, g->queue, qh, s.cfg, s.blocks, s.warps_per_block, st);
+  if (ms) cudaEventRecord(ev1, st);
+  RunCtl h;
+  if (!rc) {
+    e = cudaMemcpyAsync(&h, g->ctl, sizeof h, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = cuda_err(e, "match kernel");
+  }
+  if (!rc && ms) {
+    e = cudaEventElapsedTime(ms, ev0, ev1);
+    if (e != cudaSuccess) rc = cuda_err(e, "cudaEventElapsedTime");
+  }
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (rc) return rc;
+  if (h.error == TDFS_ERR_TIMEOUT) return fail(TDFS_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (h.error) return fail(h.error, "device error %d", h.error);
+  *raw = h.count;
+  return TDFS_OK;
+}
+
+}  // namespace
+}  // namespace tdfs
+
+using namespace tdfs;
+
+extern "C" {
+
+const char *tdfs_last_error(void) { return g_error.c_str(); }
+
+int tdfs_version(void) { return 1; }
+
+void tdfs_options_default(tdfs_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->steal = -1;
+  o->edge_end = -1;
+  o->edge_stride = 1;
+}
+
+int tdfs_graph_open(const char *prefix, int labeled, int device, tdfs_graph **out) {
+  if (!prefix || !out) return fail(TDFS_ERR_ARG, "null argument");
+  tdfs_csr *c = nullptr;
+  int rc = tdfs_csr_read(prefix, labeled, &c);
+  if (rc) return rc;
+  rc = graph_upload(c->n, c->nedges, c->rowptr.data(), c->colidx.data(), labeled ? c->labels.data() : nullptr,
+                    device, c->max_degree, out);
+  delete c;
+  return rc;
+}
+
+int tdfs_graph_from_csr(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx,
+                        const int32_t *labels, int device, tdfs_graph **out) {
+  if (!rowptr || (!colidx && nedges) || !out) return fail(TDFS_ERR_ARG, "null argument");
+  int32_t md = 0;
+  int rc = validate_csr(n, nedges, rowptr, colidx, &md);
+  if (rc) return rc;
+  return graph_upload(n, nedges, rowptr, colidx, labels, device, md, out);
+}
+
+int tdfs_graph_info(const tdfs_graph *g, int64_t *n, int64_t *nedges, int32_t *max_degree, int *labeled,
+                    size_t *device_bytes) {
+  if (!g) return fail(TDFS_ERR_ARG, "null graph");
+  if (n) *n = g->n;
+  if (nedges) *nedges = g->nedges;
+  if (max_degree) *max_degree = g->max_degree;
+  if (labeled) *labeled = g->labeled;
+  if (device_bytes) *device_bytes = g->bytes;
+  return TDFS_OK;
+}
+
+int tdfs_graph_free(tdfs_graph *g) {
+  graph_release(g);
+  return TDFS_OK;
+}
+
+int tdfs_plan_from_text(const char *text, int labeled, tdfs_plan **out) {
+  if (!text || !out) return fail(TDFS_ERR_ARG, "null argument");
+  auto p = std::make_unique<tdfs_plan>();
+  int rc = compile_pattern(text, labeled != 0, &p->host);
+  if (rc) return rc;
+  p->dev = p->host.to_device();
+  *out = p.release();
+  return TDFS_OK;
+}
+
+int tdfs_plan_compile(const char *gpath, int labeled, tdfs_plan **out) {
+  if (!gpath || !out) return fail(TDFS_ERR_ARG, "null argument");
+  std::ifstream f(gpath);
+  if (!f) return fail(TDFS_ERR_IO, "cannot open %s", gpath);
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return tdfs_plan_from_text(ss.str().c_str(), labeled, out);
+}
+
+int tdfs_plan_dump(const tdfs_plan *p, char *buf, size_t cap, size_t *len) {
+  if (!p) return fail(TDFS_ERR_ARG, "null plan");
+  const std::string s = p->host.dump_json();
+  if (len) *len = s.size() + 1;
+  if (buf && cap) {
+    const size_t n = std::min(cap - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+    if (n < s.size()) return fail(TDFS_ERR_ARG, "buffer too small (%zu needed)", s.size() + 1);
+  }
+  return TDFS_OK;
+}
+
+int tdfs_plan_info(const tdfs_plan *p, int *k, int *labeled, int64_t *multiplicity) {
+  if (!p) return fail(TDFS_ERR_ARG, "null plan");
+  if (k) *k = p->host.k;
+  if (labeled) *labeled = p->host.labeled;
+  if (multiplicity) *multiplicity = p->host.multiplicity;
+  return TDFS_OK;
+}
+
+int tdfs_plan_free(tdfs_plan *p) {
+  delete p;
+  return TDFS_OK;
+}
+
+int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint64_t *count, float *kernel_ms) {
+  if (!g || !p || !count) return fail(TDFS_ERR_ARG, "null argument");
+  tdfs_options o;
+  if (opt) o = *opt; else tdfs_options_default(&o);
+  unsigned long long raw = 0;
+  int rc = run_one(g, p->dev, o, &raw, kernel_ms);
+  if (rc) return rc;
+  // cu_test.cu:100-105: the unlabeled total is multiplied by |Aut|
+  *count = (uint64_t)(raw * (unsigned long long)p->dev.multiplicity);
+  return TDFS_OK;
+}
+
+int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *opt,
+                     uint64_t *counts, float *kernel_ms) {
+  if (!g || (!plans && nplans) || (!counts && nplans) || nplans < 0) return fail(TDFS_ERR_ARG, "bad arguments");
+  float total = 0.f;
+  for (int i = 0; i < nplans; ++i) {
+    float ms = 0.f;
+    int rc = tdfs_count(g, plans[i], opt, &counts[i], kernel_ms ? &ms : nullptr);
+    if (rc) return rc;
+    total += ms;
+  }
+  if (kernel_ms) *kernel_ms = total;
+  return TDFS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,771 @@
+// match.cu -- the sm_100a DFS subgraph-counting kernel (design notes in
+// match.cuh).  Count semantics follow src/gpu_match.cu and cu_test.cu:
+//   unlabeled: edges (r, c) with r < c when vertices 0 and 1 are symmetric,
+//              every later vertex i drawn from the intersection of its
+//              backward neighbours' lists, phi(j) < phi(i) for each
+//              symmetry pair (j, i) and phi(j) != phi(i) for other j < i;
+//              the host multiplies the total by |Aut|.
+//   labeled:   vertex labels must match and every vertex differs from all
+//              earlier ones; no multiplier.
+//   both:      the level-0 degree filter of get_job (src/gpu_match.cu:540-548).
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstdio>
+
+#include "match.cuh"
+
+namespace tdfs {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kMaxLists = kMaxK - 1;
+constexpr int kCasLimit = 1 << 20;
+constexpr int kStoredMax = kMaxK;  // level index bound (stored levels are 2..k-2)
+
+struct LevelHdr {
+  const int32_t *src;            // source list: global adjacency list or an smem buffer
+  const int32_t *mlist[kMaxLists];
+  int32_t mlen[kMaxLists];
+  int32_t mcur[kMaxLists];
+  int32_t spos, send;            // source cursor
+  int32_t lo, hi;                // x > lo, x < hi (unlabeled)
+  int32_t nm;                    // membership lists
+  int32_t nneq;
+  int32_t neqv[kMaxK];           // excluded vertices
+  int32_t nprod;                 // candidates produced into the buffer (first fill)
+  int32_t complete;              // buffer holds the whole candidate set
+  uint32_t merge_mask;           // bit m: list m uses the staged-window merge
+  int32_t pad_;
+};
+
+struct alignas(16) WarpSmem {
+  unsigned long long word[kStoredMax];  // per stored level: gen:32 | next:16 | end:16
+  int32_t phi[kMaxK + 1];
+  int32_t er[kEdgeChunk];
+  int32_t ec[kEdgeChunk];
+  int32_t en, eit;
+  int32_t pad_[2];
+  LevelHdr h[kMaxK];
+};
+
+__device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+__device__ __forceinline__ void raise_error(RunCtl *ctl, int code) { atomicCAS(&ctl->error, 0, code); }
+
+// first index in a[lo, hi) with a[idx] >= x
+__device__ __forceinline__ int32_t lower_bound(const int32_t *a, int32_t lo, int32_t hi, int32_t x) {
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// first index in a[lo, hi) with a[idx] > x, by 32-ary warp search
+__device__ int32_t warp_upper_bound(const int32_t *a, int32_t lo, int32_t hi, int32_t x) {
+  const int lane = lane_id();
+  while (hi - lo > 32) {
+    const int32_t step = (hi - lo + 31) >> 5;
+    const int32_t idx = lo + lane * step;
+    const bool le = idx < hi && a[idx] <= x;
+    const int c = __popc(__ballot_sync(kFull, le));
+    if (c == 0) return lo;
+    const int32_t nlo = lo + (c - 1) * step + 1;
+    hi = min(hi, lo + c * step);
+    lo = nlo;
+  }
+  const int32_t idx = lo + lane;
+  const bool le = idx < hi && a[idx] <= x;
+  return lo + __popc(__ballot_sync(kFull, le));
+}
+
+template <bool LAB>
+__device__ __forceinline__ bool pass_filter(int32_t x, const LevelHdr &H, int i, const DevPlan &P,
+                                            const DevGraph &G) {
+  if (LAB) {
+    if ((int32_t)G.label[x] != P.label[i]) return false;
+  } else {
+    if (x <= H.lo || x >= H.hi) return false;
+  }
+#pragma unroll
+  for (int t = 0; t < kMaxK; ++t)
+    if (t < H.nneq && H.neqv[t] == x) return false;
+  return true;
+}
+
+// Membership of each lane's x in the level's other lists.  `ok` lanes are
+// tested; cursors advance monotonically (the source is sorted).  `win` is the
+// warp's staging area for the merge path.
+__device__ __forceinline__ bool test_lists(bool ok, int32_t x, const LevelHdr &H,
+                                           int32_t (&cur)[kMaxLists], int32_t *win, int window,
+                                           const int32_t *colidx) {
+  const int lane = lane_id();
+#pragma unroll
+  for (int m = 0; m < kMaxLists; ++m) {
+    if (m >= H.nm) break;
+    const int32_t *L = H.mlist[m];
+    const int32_t len = H.mlen[m];
+    int32_t p = 0;
+    const bool searched = ok;
+    if ((H.merge_mask >> m & 1) && __any_sync(kFull, ok)) {
+      // stage L[cur .. cur + window) (16-byte aligned) in shared memory
+      const int64_t off = (int64_t)(L - colidx) + cur[m];
+      const int64_t a0 = off & ~(int64_t)3;
+      const int4 *gsrc = reinterpret_cast<const int4 *>(colidx + a0);
+      for (int t = lane; t < (window >> 2); t += 32) reinterpret_cast<int4 *>(win)[t] = __ldg(gsrc + t);
+      __syncwarp();
+      // window covers global offsets [a0, a0 + window) intersected with the list
+      const int32_t first = (int32_t)(off - a0);                      // index of cur in win
+      const int64_t lend = (int64_t)(L - colidx) + len;
+      const int64_t wend = lend - a0;
+      const int32_t last = (int32_t)(wend < (int64_t)window ? wend : (int64_t)window);  // exclusive
+      if (ok) {
+        if (first < last && x <= win[last - 1]) {
+          const int32_t q = lower_bound(win, first, last, x);
+          p = cur[m] + (q - first);
+          ok = win[q] == x;
+        } else {
+          const int32_t from = cur[m] + max(0, last - first);
+          p = lower_bound(L, from, len, x);
+          ok = p < len && L[p] == x;
+        }
+      }
+      __syncwarp();
+    } else if (ok) {
+      p = lower_bound(L, cur[m], len, x);
+      ok = p < len && L[p] == x;
+    }
+    const unsigned mx = __reduce_max_sync(kFull, searched ? (unsigned)p : 0u);
+    cur[m] = max(cur[m], (int32_t)mx);
+  }
+  return ok;
+}
+
+template <bool LAB>
+struct Engine {
+  const DevPlan &P;
+  const DevGraph &G;
+  const KernelCfg &cfg;
+  RunCtl *ctl;
+  SplitUnit *units;
+  QueueHdr *qh;
+  WarpSmem &W;
+  int32_t *bufs;  // stored level l at bufs + (l - 2) * cap
+  int32_t *win;   // merge staging (cfg.window ints)
+  unsigned char *cta;   // this CTA's shared memory (warp regions cfg.warp_bytes apart)
+  size_t hdr_bytes;     // WarpSmem rounded to 16 bytes
+  unsigned long long count = 0;
+  int lane;
+
+  __device__ Engine(const DevPlan &p, const DevGraph &g, const KernelCfg &c, RunCtl *ct, SplitUnit *u,
+                    QueueHdr *q, WarpSmem &w, int32_t *b, int32_t *wn)
+      : P(p), G(g), cfg(c), ctl(ct), units(u), qh(q), W(w), bufs(b), win(wn), lane(lane_id()) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cta = smem;
+    hdr_bytes = (sizeof(WarpSmem) + 15) & ~(size_t)15;
+  }
+
+  __device__ __forceinline__ int32_t *buf(int l) { return bufs + (l - 2) * cfg.cap; }
+  __device__ __forceinline__ int64_t deg(int32_t v) { return G.rowptr[v + 1] - G.rowptr[v]; }
+
+  // Set up the candidate scan of pattern vertex i from phi(0..i-1).
+  __device__ void setup(int i, bool allow_reuse) {
+    LevelHdr &H = W.h[i];
+    const int dep = P.dep[i];
+    const bool reuse = allow_reuse && dep >= 2 && W.h[dep].complete;
+    const int32_t *src;
+    int32_t slen;
+    int nm = 0;
+    int mylen = -1, myslot = -1;  // this lane's membership list, if any
+    if (reuse) {
+      src = buf(dep);
+      slen = W.h[dep].nprod;
+      nm = P.nsh[i];
+      if (lane < nm) {
+        const int32_t v = W.phi[P.bnsh[i][lane]];
+        const int64_t b = G.rowptr[v];
+        mylen = (int32_t)(G.rowptr[v + 1] - b);
+        myslot = lane;
+        H.mlist[lane] = G.colidx + b;
+        H.mlen[lane] = mylen;
+        H.mcur[lane] = 0;
+      }
+    } else {
+      // scan the smallest backward-neighbour list (first on ties, as
+      // src/gpu_match.cu:646-663)
+      const int nbn = P.nbn[i];
+      unsigned long long key = ~0ull;
+      int64_t b = 0, e = 0;
+      if (lane < nbn) {
+        const int32_t v = W.phi[P.bn[i][lane]];
+        b = G.rowptr[v];
+        e = G.rowptr[v + 1];
+        key = ((unsigned long long)(e - b) << 8) | (unsigned)lane;
+      }
+      unsigned long long best = key;
+#pragma unroll
+      for (int s = 16; s >= 1; s >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(kFull, best, s);
+        best = o < best ? o : best;
+      }
+      const int bmin = (int)(best & 0xff);
+      const int64_t sb = __shfl_sync(kFull, b, bmin);
+      slen = (int32_t)(best >> 8);
+      src = G.colidx + sb;
+      nm = nbn - 1;
+      if (lane < nbn && lane != bmin) {
+        myslot = lane < bmin ? lane : lane - 1;
+        mylen = (int32_t)(e - b);
+        H.mlist[myslot] = G.colidx + b;
+        H.mlen[myslot] = mylen;
+        H.mcur[myslot] = 0;
+      }
+    }
+    int32_t lo = -1, hi = INT_MAX, nneq = 0;
+    int32_t neq[kMaxK];
+#pragma unroll
+    for (int j = 0; j < kMaxK; ++j) {
+      if (j >= i) break;
+      const int32_t v = W.phi[j];
+      if (LAB) {
+        neq[nneq++] = v;
+      } else {
+        if (P.larger[i] >> j & 1) lo = max(lo, v);
+        else if (P.less[i] >> j & 1) hi = min(hi, v);
+        else neq[nneq++] = v;
+      }
+    }
+    int32_t spos = 0;
+    if (!LAB && lo >= 0 && slen > 0) spos = warp_upper_bound(src, 0, slen, lo);
+    // merge (staged window) or per-lane search, per list, by degree ratio
+    uint32_t mm = 0;
+    if (cfg.window > 0 && myslot >= 0 && (int64_t)mylen <= 4ll * max(1, slen - spos)) mm = 1u << myslot;
+    mm = __reduce_or_sync(kFull, mm);
+    if (lane == 0) {
+      H.src = src;
+      H.send = slen;
+      H.spos = spos;
+      H.lo = lo;
+      H.hi = hi;
+      H.nm = nm;
+      H.nneq = nneq;
+      for (int t = 0; t < kMaxK; ++t) H.neqv[t] = t < nneq ? neq[t] : -1;
+      H.complete = 0;
+      H.nprod = -1;
+      H.merge_mask = mm;
+    }
+    __syncwarp();
+  }
+
+  // Fill the level-i buffer with the next chunk of candidates and publish it.
+  __device__ void produce(int i) {
+    LevelHdr &H = W.h[i];
+    int32_t *out = buf(i);
+    const int32_t *src = H.src;
+    int32_t spos = H.spos;
+    const int32_t send = H.send;
+    int32_t cur[kMaxLists];
+#pragma unroll
+    for (int m = 0; m < kMaxLists; ++m) cur[m] = m < H.nm ? H.mcur[m] : 0;
+    int32_t n = 0;
+    const int32_t cap = cfg.cap;
+    while (n <= cap - 32 && spos < send) {
+      const int32_t idx = spos + lane;
+      const bool valid = idx < send;
+      const int32_t x = valid ? src[idx] : 0;
+      bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
+      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx);
+      const unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) out[n + __popc(mask & lanemask_lt())] = x;
+      n += __popc(mask);
+      spos += 32;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      const bool first = H.nprod < 0;
+      H.spos = spos;
+      for (int m = 0; m < H.nm; ++m) H.mcur[m] = cur[m];
+      if (first) {
+        H.nprod = n;
+        H.complete = spos >= send;
+      } else {
+        H.complete = 0;
+      }
+      const unsigned long long gen = (W.word[i] >> 32) + 1;
+      __threadfence_block();
+      atomicExch(&W.word[i], (gen << 32) | (unsigned long long)n);
+    }
+    __syncwarp();
+  }
+
+  // Count the candidates of the last pattern vertex (not stored).
+  __device__ unsigned long long count_last(int i) {
+    setup(i, true);
+    const LevelHdr &H = W.h[i];
+    const int32_t *src = H.src;
+    const int32_t send = H.send;
+    int32_t spos = H.spos;
+    if (!LAB && H.nm == 0 && H.hi == INT_MAX) {
+      // closed form: everything above the bound except the excluded vertices
+      int32_t hit = 0;
+      if (lane < H.nneq) {
+        const int32_t v = H.neqv[lane];
+        bool dup = false;  // equal excluded vertices are excluded once
+        for (int t = 0; t < lane; ++t) dup |= H.neqv[t] == v;
+        if (v > H.lo && !dup) {
+          const int32_t q = lower_bound(src, spos, send, v);
+          hit = q < send && src[q] == v;
+        }
+      }
+      const int32_t excl = __popc(__ballot_sync(kFull, hit));
+      return (unsigned long long)(send - spos - excl);
+    }
+    int32_t cur[kMaxLists];
+#pragma unroll
+    for (int m = 0; m < kMaxLists; ++m) cur[m] = m < H.nm ? H.mcur[m] : 0;
+    unsigned long long c = 0;
+    for (; spos < send; spos += 32) {
+      const int32_t idx = spos + lane;
+      const bool valid = idx < send;
+      const int32_t x = valid ? src[idx] : 0;
+      bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
+      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx);
+      c += __popc(__ballot_sync(kFull, ok));
+    }
+    return c;
+  }
+
+  // Claim the next buffered candidate of stored level l; -1 when none.
+  __device__ int32_t claim(int l) {
+    int32_t r = -1;
+    if (lane == 0) {
+      unsigned long long w = *(volatile unsigned long long *)&W.word[l];
+      int tries = 0;
+      for (;; ++tries) {
+        const uint32_t it = (uint32_t)(w >> 16) & 0xffffu, n = (uint32_t)w & 0xffffu;
+        if (it >= n) break;
+        if (tries >= kCasLimit) {
+          raise_error(ctl, TDFS_ERR_TIMEOUT);
+          break;
+        }
+        const unsigned long long old = atomicCAS(&W.word[l], w, w + (1ull << 16));
+        if (old == w) {
+          r = (int32_t)it;
+          break;
+        }
+        w = old;
+      }
+    }
+    return __shfl_sync(kFull, r, 0);
+  }
+
+  // Level-0 chunk: up to 32 directed edges, filtered as get_job
+  // (src/gpu_match.cu:531-556).  Returns false once the edge range is spent.
+  __device__ bool fetch_edges() {
+    for (;;) {
+      unsigned long long t = 0;
+      if (lane == 0) t = atomicAdd(&ctl->edge_next, 1ull);
+      t = __shfl_sync(kFull, t, 0);
+      const int64_t e0 = cfg.e_begin + ((int64_t)t * cfg.stride + cfg.phase) * kEdgeChunk;
+      if (e0 >= cfg.e_end) return false;
+      const int64_t e = e0 + lane;
+      bool ok = e < cfg.e_end;
+      int32_t r = 0, c = 0;
+      if (ok) {
+        r = G.src[e];
+        c = G.colidx[e];
+        if (!LAB && P.orient && !(r < c)) ok = false;
+        if (LAB && ok && ((int32_t)G.label[r] != P.label[0] || (int32_t)G.label[c] != P.label[1])) ok = false;
+        if (ok && (deg(r) < P.deg[0] || deg(c) < P.deg[1] || G.maxnd[c] < P.deg[2])) ok = false;
+      }
+      const unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) {
+        const int slot = __popc(mask & lanemask_lt());
+        W.er[slot] = r;
+        W.ec[slot] = c;
+      }
+      if (lane == 0) {
+        W.en = __popc(mask);
+        W.eit = 0;
+      }
+      __syncwarp();
+      if (mask) return true;
+    }
+  }
+
+  // ---- work stealing and the global split queue ---------------------------
+
+  __device__ __forceinline__ WarpSmem &warp_at(int v) {
+    return *reinterpret_cast<WarpSmem *>(cta + (size_t)v * cfg.warp_bytes);
+  }
+  __device__ __forceinline__ int32_t *buf_of(int v, int l) {
+    return reinterpret_cast<int32_t *>(cta + (size_t)v * cfg.warp_bytes + hdr_bytes) + cfg.window +
+           (l - 2) * cfg.cap;
+  }
+
+  // Publish `cnt` candidates of vertex l (already in this warp's level-l
+  // buffer, prefix already in W.phi) as this warp's new base subtree.
+  __device__ void install(int l, int cnt) {
+    if (lane == 0) {
+      for (int j = 2; j <= l; ++j) W.h[j].complete = 0;
+      W.h[l].spos = W.h[l].send = 0;  // no source left: only the given candidates
+      W.h[l].nprod = cnt;
+      const unsigned long long gen = (W.word[l] >> 32) + 1;
+      __threadfence_block();
+      atomicExch(&W.word[l], (gen << 32) | (unsigned long long)cnt);
+    }
+    __syncwarp();
+  }
+
+  // Steal half of the remaining candidates at the shallowest stored level of
+  // another warp of this CTA.  The thief copies the victim's prefix and the
+  // upper half of its buffered candidates, then CASes the victim's word
+  // (gen | next | end) to lower `end`; the copy is valid iff the CAS succeeds,
+  // because the victim only rewrites its buffer or prefix after bumping gen.
+  // Returns the level or 0.
+  __device__ int steal_local(int nwarps, int me) {
+    const int k = P.k;
+    for (int l = 2; l <= k - 2; ++l) {
+      int rem = 0, vic = -1;
+      if (lane < nwarps && lane != me) {
+        const unsigned long long w = *(volatile unsigned long long *)&warp_at(lane).word[l];
+        rem = (int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu);
+        vic = lane;
+      }
+      unsigned long long key = ((unsigned long long)(unsigned)max(rem, 0) << 32) | (unsigned)(vic + 1);
+#pragma unroll
+      for (int s = 16; s >= 1; s >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(kFull, key, s);
+        key = o > key ? o : key;
+      }
+      if ((int)(key >> 32) < 2) continue;
+      vic = (int)(key & 0xffffffffu) - 1;
+      WarpSmem &V = warp_at(vic);
+      unsigned long long w = 0;
+      if (lane == 0) w = *(volatile unsigned long long *)&V.word[l];
+      w = __shfl_sync(kFull, w, 0);
+      __threadfence_block();
+      const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
+      if (n - it < 2) continue;
+      const int take = (n - it) / 2;
+      const int from = n - take;
+      const volatile int32_t *vb = buf_of(vic, l);
+      int32_t *mb = buf(l);
+      for (int t = lane; t < take; t += 32) mb[t] = vb[from + t];
+      if (lane < l) W.phi[lane] = ((volatile int32_t *)V.phi)[lane];
+      __threadfence_block();
+      __syncwarp();
+      int won = 0;
+      if (lane == 0) won = atomicCAS(&V.word[l], w, (w & ~0xffffull) | (unsigned long long)from) == w;
+      won = __shfl_sync(kFull, won, 0);
+      if (won) {
+        install(l, take);
+        if (lane == 0) atomicAdd(&ctl->steals, 1ull);
+        return l;
+      }
+    }
+    return 0;
+  }
+
+  // Bounded MPMC ring with per-slot sequence numbers (lane 0 only).  A slot
+  // is reserved before its unit is written, so a donation can never be left
+  // without a place; consumers skip units with no items.
+  __device__ long long queue_reserve() {
+    unsigned long long pos = *(volatile unsigned long long *)&qh->tail;
+    for (int tries = 0; tries < 64; ++tries) {
+      const unsigned long long seq = *(volatile unsigned long long *)&qh->seq[pos & (kQueueCap - 1)];
+      const long long dif = (long long)(seq - pos);
+      if (dif == 0) {
+        const unsigned long long old = atomicCAS(&qh->tail, pos, pos + 1);
+        if (old == pos) return (long long)pos;
+        pos = old;
+      } else if (dif < 0) {
+        return -1;  // full
+      } else {
+        pos = *(volatile unsigned long long *)&qh->tail;
+      }
+    }
+    return -1;
+  }
+
+  __device__ void queue_publish(unsigned long long pos, int l, const int32_t *items, int cnt) {
+    SplitUnit &u = units[pos & (kQueueCap - 1)];
+    u.level = l;
+    u.nitems = cnt;
+    for (int j = 0; j < l; ++j) u.phi[j] = W.phi[j];
+    for (int t = 0; t < cnt; ++t) u.items[t] = items[t];
+    __threadfence();
+    atomicExch(&qh->seq[pos & (kQueueCap - 1)], pos + 1);
+  }
+
+  // Pop one unit into this warp's state; returns its level or 0.
+  __device__ int queue_pop() {
+    int l = 0, cnt = 0;
+    if (lane == 0) {
+      unsigned long long pos = *(volatile unsigned long long *)&qh->head;
+      for (int tries = 0; tries < 64; ++tries) {
+        const unsigned long long slot = pos & (kQueueCap - 1);
+        const unsigned long long seq = *(volatile unsigned long long *)&qh->seq[slot];
+        const long long dif = (long long)(seq - (pos + 1));
+        if (dif == 0) {
+          const unsigned long long old = atomicCAS(&qh->head, pos, pos + 1);
+          if (old == pos) {
+            __threadfence();
+            const volatile SplitUnit &u = units[slot];
+            l = u.level;
+            cnt = u.nitems;
+            if (l >= 2 && l <= P.k - 2 && cnt > 0 && cnt <= kUnitItems) {
+              for (int j = 0; j < l; ++j) W.phi[j] = u.phi[j];
+              int32_t *mb = buf(l);
+              for (int t = 0; t < cnt; ++t) mb[t] = u.items[t];
+            } else {
+              l = 0;
+            }
+            __threadfence();
+            atomicExch(&qh->seq[slot], pos + kQueueCap);
+            break;
+          }
+          pos = old;
+        } else if (dif < 0) {
+          break;  // empty
+        } else {
+          pos = *(volatile unsigned long long *)&qh->head;
+        }
+      }
+    }
+    l = __shfl_sync(kFull, l, 0);
+    cnt = __shfl_sync(kFull, cnt, 0);
+    __syncwarp();
+    if (!l) return 0;
+    install(l, cnt);
+    return l;
+  }
+
+  // Busy warp: when some warp is hungry, move up to kUnitItems of the
+  // shallowest remaining candidates into the global ring.
+  __device__ void maybe_donate(int level) {
+    int hungry = 0;
+    if (lane == 0) hungry = *(volatile int32_t *)&ctl->hungry;
+    hungry = __shfl_sync(kFull, hungry, 0);
+    if (hungry <= 0) return;
+    if (lane == 0) {
+      int l = 2;
+      for (; l <= level; ++l) {
+        const unsigned long long w = *(volatile unsigned long long *)&W.word[l];
+        if ((int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu) >= 2) break;
+      }
+      if (l <= level) {
+        const long long pos = queue_reserve();
+        if (pos >= 0) {
+          int cnt = 0, from = 0;
+          unsigned long long w = *(volatile unsigned long long *)&W.word[l];
+          for (int t = 0; t < kCasLimit; ++t) {
+            const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
+            if (n - it < 2) break;
+            const int take = min((n - it) / 2, kUnitItems);
+            const unsigned long long old = atomicCAS(&W.word[l], w, (w & ~0xffffull) | (unsigned long long)(n - take));
+            if (old == w) {
+              cnt = take;
+              from = n - take;
+              break;
+            }
+            w = old;
+          }
+          queue_publish((unsigned long long)pos, l, buf(l) + from, cnt);
+          if (cnt) atomicAdd(&ctl->splits, 1ull);
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  // ---- main loop ------------------------------------------------------------
+  __device__ void run(int nwarps, int me) {
+    const int k = P.k;
+    int level = 1, base = 1;
+    bool edges_left = true;
+    bool busy = true;   // counted in ctl->pending
+    bool hungry = false;  // counted in ctl->hungry
+    unsigned claims = 0;
+    if (lane == 0) {
+      W.en = W.eit = 0;
+      for (int l = 0; l < kStoredMax; ++l) W.word[l] = 0;
+      for (int l = 0; l < kMaxK; ++l) W.h[l].complete = 0;
+    }
+    __syncwarp();
+    for (;;) {
+      if (level < base) {
+        // ---- acquire new work: edges, then a local steal, then the ring ----
+        level = 0;
+        if (edges_left) {
+          if (fetch_edges()) level = base = 1;
+          else edges_left = false;
+        }
+        if (!level && cfg.steal) {
+          for (int polls = 0;; ++polls) {
+            int l = steal_local(nwarps, me);
+            if (!l) l = queue_pop();
+            if (l) {
+              level = base = l;
+              break;
+            }
+            if (lane == 0) {
+              if (busy) atomicSub(&ctl->pending, 1);
+              if (!hungry) atomicAdd(&ctl->hungry, 1);
+            }
+            busy = false;
+            hungry = true;
+            int done = 0;
+            if (lane == 0) {
+              const int pend = *(volatile int32_t *)&ctl->pending;
+              const unsigned long long h = *(volatile unsigned long long *)&qh->head;
+              const unsigned long long t = *(volatile unsigned long long *)&qh->tail;
+              done = pend <= 0 && h == t;
+            }
+            done = __shfl_sync(kFull, done, 0);
+            // retiring early is safe: every unit is pushed by a busy warp,
+            // which drains the ring itself before it retires
+            if (done || polls >= cfg.poll_limit) break;
+            __nanosleep(polls < 64 ? 256 : 2048);
+          }
+          if (level && lane == 0) {
+            if (!busy) atomicAdd(&ctl->pending, 1);
+            if (hungry) atomicSub(&ctl->hungry, 1);
+          }
+          if (level) {
+            busy = true;
+            hungry = false;
+          }
+        }
+        if (!level) break;
+        continue;
+      }
+      if (level == 1) {
+        if (W.eit >= W.en) {
+          level = 0;  // chunk spent: acquire more
+          base = 1;
+          continue;
+        }
+        const int t = W.eit;
+        const int32_t r = W.er[t], c = W.ec[t];
+        __syncwarp();
+        if (lane == 0) {
+          W.eit = t + 1;
+          W.phi[0] = r;
+          W.phi[1] = c;
+        }
+        __syncwarp();
+        if (k == 3) {
+          count += count_last(2);
+        } else {
+          setup(2, true);
+          produce(2);
+          level = 2;
+        }
+        continue;
+      }
+      // stored level 2 <= level <= k-2
+      const int32_t idx = claim(level);
+      if (idx >= 0) {
+        const int32_t x = buf(level)[idx];
+        __syncwarp();
+        if (lane == 0) W.phi[level] = x;
+        __syncwarp();
+        if (cfg.steal && ((++claims & 15u) == 0)) maybe_donate(level);
+        if (level + 1 == k - 1) {
+          count += count_last(k - 1);
+        } else {
+          setup(level + 1, true);
+          produce(level + 1);
+          ++level;
+        }
+        continue;
+      }
+      if (W.h[level].spos < W.h[level].send) {
+        produce(level);
+        continue;
+      }
+      --level;
+    }
+    if (lane == 0 && cfg.steal) {
+      if (busy) atomicSub(&ctl->pending, 1);
+      if (hungry) atomicSub(&ctl->hungry, 1);
+    }
+    __syncwarp();
+  }
+};
+
+template <bool LAB>
+__global__ void __launch_bounds__(256) match_kernel(const __grid_constant__ DevPlan P,
+                                                    const __grid_constant__ DevGraph G,
+                                                    const __grid_constant__ KernelCfg cfg, RunCtl *ctl,
+                                                    SplitUnit *units, QueueHdr *qh) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int me = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  unsigned char *base = smem + (size_t)me * cfg.warp_bytes;
+  WarpSmem &W = *reinterpret_cast<WarpSmem *>(base);
+  const size_t hdr = (sizeof(WarpSmem) + 15) & ~(size_t)15;
+  int32_t *win = reinterpret_cast<int32_t *>(base + hdr);
+  int32_t *bufs = win + cfg.window;
+  Engine<LAB> eng(P, G, cfg, ctl, units, qh, W, bufs, win);
+  eng.run(nwarps, me);
+  unsigned long long c = eng.count;
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&ctl->count, c);
+}
+
+__global__ void init_kernel(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t == 0) {
+    ctl->edge_next = 0;
+    ctl->count = 0;
+    ctl->steals = 0;
+    ctl->splits = 0;
+    ctl->error = 0;
+    ctl->pending = total_warps;
+    ctl->hungry = 0;
+    qh->head = 0;
+    qh->tail = 0;
+  }
+  for (int i = t; i < kQueueCap; i += gridDim.x * blockDim.x) qh->seq[i] = (unsigned long long)i;
+  (void)e_begin;
+}
+
+}  // namespace
+
+size_t warp_smem_bytes(int k, int cap, int window) {
+  const size_t hdr = (sizeof(WarpSmem) + 15) & ~(size_t)15;
+  const int stored = k > 3 ? k - 3 : 0;
+  return hdr + sizeof(int32_t) * ((size_t)window + (size_t)stored * cap);
+}
+
+void init_launch(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin, cudaStream_t stream) {
+  init_kernel<<<64, 256, 0, stream>>>(ctl, qh, total_warps, e_begin);
+}
+
+int launch_match(const DevPlan &plan, const DevGraph &g, RunCtl *ctl, SplitUnit *units, QueueHdr *qh,
+                 const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream) {
+  const size_t smem = (size_t)cfg.warp_bytes * warps_per_block;
+  cudaError_t e;
+  if (plan.labeled) {
+    e = cudaFuncSetAttribute(match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      match_kernel<true><<<blocks, warps_per_block * 32, smem, stream>>>(plan, g, cfg, ctl, units, qh);
+  } else {
+    e = cudaFuncSetAttribute(match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      match_kernel<false><<<blocks, warps_per_block * 32, smem, stream>>>(plan, g, cfg, ctl, units, qh);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "match kernel launch: %s", cudaGetErrorString(e));
+  return TDFS_OK;
+}
+
+}  // namespace tdfs

@@ -1,0 +1,66 @@
+// match.cuh -- the sm_100a DFS subgraph-counting kernel.
+//
+// Replaces the reference kernel _parallel_match (src/gpu_match.cu:951-1080)
+// with the same count semantics and a different execution design:
+//
+//  * Persistent grid, one warp per DFS.  The plan is a __grid_constant__
+//    parameter (constant bank); per-warp state and the candidate buffers of
+//    every stored level live in shared memory, not in a 240 KB/warp global
+//    stack (src/callstack.h, cu_test.cu:36-49).
+//  * Candidate sets are produced in bounded chunks of `cap` vertices from a
+//    resumable source cursor, so a hub's candidate set never overflows a
+//    buffer (the reference writes past GRAPH_DEGREE=4096, src/config.h:12).
+//  * One scan produces the set directly as filter(source) ∩ other lists:
+//    the symmetry conditions become a lower bound (the source is sorted, so
+//    the prefix below it is skipped by a 32-ary warp search) plus at most six
+//    inequality tests; labels and injectivity are fused into the same pass
+//    (src/gpu_match.cu:260-494 does this as separate passes through global
+//    memory).
+//  * Membership is tested with per-lane searches from a monotone cursor, or by
+//    staging the matching window of the other list in shared memory with
+//    16-byte loads (merge), picked per 32-element step by how wide the window
+//    is, i.e. by the local degree ratio.
+//  * The last pattern vertex is only counted (ballot + popc); a last vertex
+//    with a single backward neighbour and no label test is counted in closed
+//    form from the bound and the excluded vertices.
+//  * Load balance: level-0 edge chunks from an atomic ticket (as get_job,
+//    src/gpu_match.cu:496-569, but one edge per lane and the neighbour-degree
+//    test precomputed); idle warps steal half of another warp's buffered
+//    candidates at its shallowest level through 64-bit shared-memory words
+//    (gen | next | end) and CAS; busy warps donate candidates to a bounded
+//    lock-free ring in HBM when warps anywhere are hungry (the reference's
+//    timeout queue, src/queue.h, src/gpu_match.cu:875-909).  Every wait is
+//    bounded and reports TDFS_ERR_TIMEOUT through RunCtl::error.
+#pragma once
+
+#include <cstdint>
+
+#include "common.h"
+#include "graph.h"
+
+namespace tdfs {
+
+struct KernelCfg {
+  int64_t e_begin;      // level-0 edge range
+  int64_t e_end;
+  int32_t stride;       // chunks dealt round-robin over `stride` shards
+  int32_t phase;        // this launch's shard
+  int32_t cap;          // candidates per stored level (multiple of 32)
+  int32_t warp_bytes;   // shared memory per warp
+  int32_t steal;        // 1: stealing + donation on
+  int32_t window;       // merge window in ints (multiple of 128) or 0 = off
+  int32_t poll_limit;   // idle polls before a warp retires
+  int32_t pad_;
+};
+
+constexpr int kEdgeChunk = 32;  // directed edges per level-0 ticket
+
+size_t warp_smem_bytes(int k, int cap, int window);
+
+// Launch the counting kernel for one plan.  `ctl` must have been initialised
+// by init_launch on the same stream.
+int launch_match(const DevPlan &plan, const DevGraph &g, RunCtl *ctl, SplitUnit *units, QueueHdr *qh,
+                 const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream);
+void init_launch(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin, cudaStream_t stream);
+
+}  // namespace tdfs

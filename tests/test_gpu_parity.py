@@ -1,0 +1,162 @@
+"""GPU counts through the C ABI vs the CPU oracle, bit-exact (uint64).
+
+Graphs are the seeded synthetic inputs of the benchmark configs at sizes the
+oracle finishes in seconds: the ER graph of the small configs at full size
+(n=4096, average degree 16, seed 0; labels uniform in [0,4), seed 2),
+reduced Chung-Lu power-law graphs (hubs far above the per-level buffer so
+chunked production, stealing and the split queue all run), a reduced R-MAT
+graph, and complete graphs with closed-form counts."""
+import json
+import math
+import os
+import random
+
+import numpy as np
+import pytest
+
+from tests.golden.make_golden import random_pattern
+from tests.patterns import CYCLE4, HOUSE, TRIANGLE, clique, reference_patterns
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+OPTION_SETS = [
+    {},                                              # defaults (stealing + split queue on, merge window)
+    {"steal": 0},                                    # plain persistent DFS
+    {"merge_window": -1},                            # per-lane search only
+    {"chunk_cap": 64, "warps_per_block": 4},         # tiny buffers: many refills
+    {"merge_window": 256, "chunk_cap": 128, "blocks_per_sm": 1},
+]
+
+
+class Case:
+    def __init__(self, T, po, csr, labeled):
+        self.csr = csr
+        self.dev = T.GraphPreprocessor(csr=csr, labeled=labeled)
+        self.ora = po.Graph(csr.rowptr.copy(), csr.colidx.copy(),
+                            None if csr.labels is None else csr.labels.copy())
+        self.T, self.po = T, po
+
+    def check(self, text, labeled, **opt):
+        T, po = self.T, self.po
+        want = po.count(self.ora, po.Plan(text, labeled))
+        got = T.count(self.dev, T.PatternPreprocessor(text=text, labeled=labeled), T.default_options(**opt))
+        assert got.count == want, (text, labeled, opt, got.count, want)
+        return want
+
+
+@pytest.fixture(scope="module")
+def er(T, po):
+    return Case(T, po, T.gen_er(4096, 16.0, 0).set_labels(4, 2), True)
+
+
+@pytest.fixture(scope="module")
+def cl(T, po):
+    # reduced Chung-Lu: 50k vertices, 150k edges, gamma 2.1, cap 3000 (max degree ~2.2k > buffers)
+    return Case(T, po, T.gen_chung_lu(50000, 150000, 2.1, 3000, 1).set_labels(4, 2), True)
+
+
+@pytest.fixture(scope="module")
+def cl_small(T, po):
+    return Case(T, po, T.gen_chung_lu(20000, 60000, 2.1, 600, 1).set_labels(4, 2), True)
+
+
+def test_er_unlabeled_config_patterns(er):
+    for text in [TRIANGLE, CYCLE4, clique(4)] + [t for _, t in reference_patterns()]:
+        assert er.check(text, False) > 0
+
+
+def test_er_labeled_reference_patterns(er):
+    for _, text in reference_patterns():
+        er.check(text, True)
+
+
+def test_er_labeled_random_6_7(er):
+    rng = random.Random(3)
+    for t in range(16):
+        er.check(random_pattern(6 + t % 2, 0.4, 4, rng), True)
+
+
+@pytest.mark.parametrize("opt", OPTION_SETS)
+def test_er_option_sets(er, opt):
+    for text in [TRIANGLE, CYCLE4, clique(4), HOUSE]:
+        er.check(text, False, **opt)
+    rng = random.Random(5)
+    for t in range(4):
+        er.check(random_pattern(5 + t % 3, 0.5, 4, rng), True, **opt)
+
+
+@pytest.mark.parametrize("opt", OPTION_SETS)
+def test_powerlaw_unlabeled(cl, opt):
+    for text in [TRIANGLE, CYCLE4, clique(4), clique(5)]:
+        cl.check(text, False, **opt)
+
+
+def test_powerlaw_house_and_reference(cl_small):
+    for text in [HOUSE] + [t for _, t in reference_patterns()]:
+        cl_small.check(text, False)
+        cl_small.check(text, True)
+
+
+def test_powerlaw_labeled_random(cl):
+    rng = random.Random(3)
+    for t in range(10):
+        cl.check(random_pattern(4 + t % 4, 0.45, 4, rng), True)
+
+
+def test_rmat_reduced(T, po):
+    case = Case(T, po, T.gen_rmat(14, 16, 0.57, 0.19, 0.19, 4), False)
+    for text in [TRIANGLE, clique(4)]:
+        case.check(text, False)
+
+
+@pytest.mark.parametrize("n", [12, 40])
+def test_complete_graph_closed_form(T, n):
+    rowptr = np.arange(0, n * (n - 1) + 1, n - 1, dtype=np.int64)
+    colidx = np.array([j for i in range(n) for j in range(n) if j != i], dtype=np.int32)
+    G = T.GraphPreprocessor(rowptr=rowptr, colidx=colidx, labels=np.ones(n, np.int32), labeled=True)
+    for k, text in [(3, TRIANGLE), (4, CYCLE4), (5, HOUSE), (5, clique(5)), (6, clique(6)), (7, clique(7))]:
+        for labeled in (False, True):
+            got = T.count(G, T.PatternPreprocessor(text=text, labeled=labeled)).count
+            assert got == math.perm(n, k)
+
+
+def test_edge_shards_sum_to_total(er, T):
+    """Level-0 chunks dealt round-robin over shards (the multi-GPU split)."""
+    P = T.PatternPreprocessor(text=clique(4))
+    total = T.count(er.dev, P).count
+    parts = [T.count(er.dev, P, T.default_options(edge_stride=3, edge_phase=r)).count for r in range(3)]
+    assert sum(parts) == total and min(parts) > 0
+
+
+def test_cli_matches_reference_line_format(T, tmp_path):
+    import subprocess
+    g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
+    prefix = str(tmp_path / "snap.txt")
+    g.write(prefix)
+    pat = tmp_path / "tri.g"
+    pat.write_text(TRIANGLE)
+    for exe, labeled in (("ulb", False), ("lb", True)):
+        out = subprocess.run([os.path.join(T.BIN_DIR, exe), prefix, str(pat)], capture_output=True, text=True,
+                             check=True).stdout.strip().splitlines()[-1]
+        path, ms, cnt = out.split("\t")
+        assert path == str(pat) and float(ms) > 0
+        G = T.GraphPreprocessor(prefix, labeled=labeled)
+        assert int(cnt) == T.count(G, T.PatternPreprocessor(str(pat), labeled)).count
+
+
+def test_reference_build_counts(T):
+    """Counts printed by the reference's own CUDA build (tests/golden/ref_counts.json)."""
+    path = os.path.join(GOLDEN, "ref_counts.json")
+    if not os.path.exists(path):
+        pytest.skip("no recorded reference counts")
+    recs = json.load(open(path))
+    graphs = {
+        "er4096_d16_s0_l4s2": T.gen_er(4096, 16.0, 0).set_labels(4, 2),
+        "chunglu20k_m60k_g2.1_cap600_s1_l4s2": T.gen_chung_lu(20000, 60000, 2.1, 600, 1).set_labels(4, 2),
+    }
+    dev = {k: T.GraphPreprocessor(csr=v, labeled=True) for k, v in graphs.items()}
+    for r in recs:
+        got = T.count(dev[r["graph"]], T.PatternPreprocessor(text=r["text"], labeled=r["labeled"])).count
+        assert got == r["count"], r
