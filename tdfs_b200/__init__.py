@@ -273,3 +273,27 @@ def count_batch(graph: GraphPreprocessor, patterns, options: Options | None = No
     _check(lib().tdfs_count_batch(graph._h, arr, len(patterns), None if options is None else C.byref(options),
                                   out, C.byref(ms)))
     return list(out), ms.value
+
+
+EDGE_CHUNK = 32  # directed edges per level-0 ticket (kEdgeChunk in match.cuh)
+
+
+def shard_options(rank: int, world: int, **kw) -> Options:
+    """Options for rank `rank` of `world` GPUs: level-0 edge chunks are dealt
+    round-robin, chunk t going to rank t % world, so the ranks' counts sum to
+    the whole count with no data-path collective (one u64 reduction)."""
+    if not 0 <= rank < world:
+        raise ValueError("rank out of range")
+    return default_options(edge_stride=world, edge_phase=rank, **kw)
+
+
+def shard_edge_ranges(nedges: int, rank: int, world: int):
+    """The [begin, end) edge ranges rank `rank` covers under shard_options."""
+    out = []
+    t = 0
+    while True:
+        b = (t * world + rank) * EDGE_CHUNK
+        if b >= nedges:
+            return out
+        out.append((b, min(nedges, b + EDGE_CHUNK)))
+        t += 1

@@ -60,9 +60,16 @@ int cuda_err(cudaError_t e, const char *what) {
 
 // Choose the launch shape: a persistent grid of (resident CTAs per SM) x SMs.
 int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, LaunchShape *out) {
-  cudaDeviceProp prop;
-  cudaError_t e = cudaGetDeviceProperties(&prop, g->device);
-  if (e != cudaSuccess) return cuda_err(e, "cudaGetDeviceProperties");
+  // device properties are queried once per device (the query costs ~ms)
+  static cudaDeviceProp props[64];
+  static bool have[64] = {};
+  if (g->device < 0 || g->device >= 64) return fail(TDFS_ERR_ARG, "device index");
+  if (!have[g->device]) {
+    cudaError_t e = cudaGetDeviceProperties(&props[g->device], g->device);
+    if (e != cudaSuccess) return cuda_err(e, "cudaGetDeviceProperties");
+    have[g->device] = true;
+  }
+  const cudaDeviceProp &prop = props[g->device];
   LaunchShape s;
   std::memset(&s, 0, sizeof s);
   s.warps_per_block = o.warps_per_block > 0 ? o.warps_per_block : 8;
@@ -77,7 +84,7 @@ int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, La
   c.window = window;
   c.warp_bytes = (int)((warp_smem_bytes(p.k, cap, window) + 15) & ~(size_t)15);
   c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
-  c.poll_limit = 4096;
+  c.idle_ms = 30000;
   c.e_begin = std::max<int64_t>(0, o.edge_begin);
   c.e_end = (o.edge_end < 0 || o.edge_end > g->nedges) ? g->nedges : o.edge_end;
   c.stride = o.edge_stride > 0 ? o.edge_stride : 1;
@@ -87,11 +94,11 @@ int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, La
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
                 smem, (size_t)prop.sharedMemPerBlockOptin);
-  int per_sm = o.blocks_per_sm;
-  if (per_sm <= 0) {
-    per_sm = (int)(prop.sharedMemPerMultiprocessor / (smem + prop.reservedSharedMemPerBlock));
-    per_sm = std::max(1, std::min(per_sm, prop.maxThreadsPerMultiProcessor / (32 * s.warps_per_block)));
-  }
+  const int fit = resident_blocks_per_sm(p.labeled != 0, s.warps_per_block, smem);
+  if (fit < 0) return fail(TDFS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+  if (fit == 0) return fail(TDFS_ERR_CAPACITY, "the match kernel does not fit on an SM with this shape");
+  // a persistent grid: every CTA resident at once (idle warps wait on busy ones)
+  int per_sm = o.blocks_per_sm > 0 ? std::min(o.blocks_per_sm, fit) : fit;
   s.blocks = prop.multiProcessorCount * per_sm;
   *out = s;
   return TDFS_OK;

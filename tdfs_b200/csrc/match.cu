@@ -41,12 +41,10 @@ struct LevelHdr {
 };
 
 struct alignas(16) WarpSmem {
-  unsigned long long word[kStoredMax];  // per stored level: gen:32 | next:16 | end:16
+  unsigned long long word[kStoredMax];  // per level 1..k-2: gen:32 | next:16 | end:16
   int32_t phi[kMaxK + 1];
-  int32_t er[kEdgeChunk];
+  int32_t er[kEdgeChunk];        // level-1 items: edge pairs (phi(0), phi(1))
   int32_t ec[kEdgeChunk];
-  int32_t en, eit;
-  int32_t pad_[2];
   LevelHdr h[kMaxK];
 };
 
@@ -367,7 +365,8 @@ struct Engine {
   }
 
   // Level-0 chunk: up to 32 directed edges, filtered as get_job
-  // (src/gpu_match.cu:531-556).  Returns false once the edge range is spent.
+  // (src/gpu_match.cu:531-556), published as this warp's level-1 items
+  // (pairs phi(0), phi(1)).  Returns false once the edge range is spent.
   __device__ bool fetch_edges() {
     for (;;) {
       unsigned long long t = 0;
@@ -391,13 +390,20 @@ struct Engine {
         W.er[slot] = r;
         W.ec[slot] = c;
       }
-      if (lane == 0) {
-        W.en = __popc(mask);
-        W.eit = 0;
-      }
       __syncwarp();
-      if (mask) return true;
+      if (mask) {
+        if (lane == 0) publish(1, __popc(mask));
+        __syncwarp();
+        return true;
+      }
     }
+  }
+
+  // New batch of `n` items at level l (1 = edge pairs, >= 2 candidates).
+  __device__ __forceinline__ void publish(int l, int n) {
+    const unsigned long long gen = (W.word[l] >> 32) + 1;
+    __threadfence_block();
+    atomicExch(&W.word[l], (gen << 32) | (unsigned long long)n);
   }
 
   // ---- work stealing and the global split queue ---------------------------
@@ -410,29 +416,29 @@ struct Engine {
            (l - 2) * cfg.cap;
   }
 
-  // Publish `cnt` candidates of vertex l (already in this warp's level-l
-  // buffer, prefix already in W.phi) as this warp's new base subtree.
+  // Make `cnt` items of level l (already in this warp's level-l storage,
+  // prefix already in W.phi) this warp's new base subtree.
   __device__ void install(int l, int cnt) {
     if (lane == 0) {
-      for (int j = 2; j <= l; ++j) W.h[j].complete = 0;
-      W.h[l].spos = W.h[l].send = 0;  // no source left: only the given candidates
-      W.h[l].nprod = cnt;
-      const unsigned long long gen = (W.word[l] >> 32) + 1;
-      __threadfence_block();
-      atomicExch(&W.word[l], (gen << 32) | (unsigned long long)cnt);
+      for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
+      if (l >= 2) {
+        W.h[l].spos = W.h[l].send = 0;  // no source left: only the given candidates
+        W.h[l].nprod = cnt;
+      }
+      publish(l, cnt);
     }
     __syncwarp();
   }
 
-  // Steal half of the remaining candidates at the shallowest stored level of
-  // another warp of this CTA.  The thief copies the victim's prefix and the
-  // upper half of its buffered candidates, then CASes the victim's word
-  // (gen | next | end) to lower `end`; the copy is valid iff the CAS succeeds,
-  // because the victim only rewrites its buffer or prefix after bumping gen.
-  // Returns the level or 0.
+  // Steal half of the remaining items at the shallowest level of another
+  // warp of this CTA.  The thief copies the victim's prefix and the upper
+  // half of its items, then CASes the victim's word (gen | next | end) down
+  // to the split point; the copy is valid iff the CAS succeeds, because the
+  // victim rewrites its items or prefix only after bumping gen.  Returns the
+  // level (1 = edge pairs) or 0.
   __device__ int steal_local(int nwarps, int me) {
     const int k = P.k;
-    for (int l = 2; l <= k - 2; ++l) {
+    for (int l = 1; l <= k - 2; ++l) {
       int rem = 0, vic = -1;
       if (lane < nwarps && lane != me) {
         const unsigned long long w = *(volatile unsigned long long *)&warp_at(lane).word[l];
@@ -456,10 +462,17 @@ struct Engine {
       if (n - it < 2) continue;
       const int take = (n - it) / 2;
       const int from = n - take;
-      const volatile int32_t *vb = buf_of(vic, l);
-      int32_t *mb = buf(l);
-      for (int t = lane; t < take; t += 32) mb[t] = vb[from + t];
-      if (lane < l) W.phi[lane] = ((volatile int32_t *)V.phi)[lane];
+      if (l == 1) {
+        if (lane < take) {
+          W.er[lane] = ((volatile int32_t *)V.er)[from + lane];
+          W.ec[lane] = ((volatile int32_t *)V.ec)[from + lane];
+        }
+      } else {
+        const volatile int32_t *vb = buf_of(vic, l);
+        int32_t *mb = buf(l);
+        for (int t = lane; t < take; t += 32) mb[t] = vb[from + t];
+        if (lane < l) W.phi[lane] = ((volatile int32_t *)V.phi)[lane];
+      }
       __threadfence_block();
       __syncwarp();
       int won = 0;
@@ -495,12 +508,22 @@ struct Engine {
     return -1;
   }
 
-  __device__ void queue_publish(unsigned long long pos, int l, const int32_t *items, int cnt) {
+  // Write a unit: level l, prefix W.phi[0..l-1], items [from, from+cnt) of
+  // level l (pairs when l == 1).
+  __device__ void queue_publish(unsigned long long pos, int l, int from, int cnt) {
     SplitUnit &u = units[pos & (kQueueCap - 1)];
     u.level = l;
     u.nitems = cnt;
-    for (int j = 0; j < l; ++j) u.phi[j] = W.phi[j];
-    for (int t = 0; t < cnt; ++t) u.items[t] = items[t];
+    if (l == 1) {
+      for (int t = 0; t < cnt; ++t) {
+        u.items[2 * t] = W.er[from + t];
+        u.items[2 * t + 1] = W.ec[from + t];
+      }
+    } else {
+      for (int j = 0; j < l; ++j) u.phi[j] = W.phi[j];
+      const int32_t *b = buf(l);
+      for (int t = 0; t < cnt; ++t) u.items[t] = b[from + t];
+    }
     __threadfence();
     atomicExch(&qh->seq[pos & (kQueueCap - 1)], pos + 1);
   }
@@ -521,7 +544,12 @@ struct Engine {
             const volatile SplitUnit &u = units[slot];
             l = u.level;
             cnt = u.nitems;
-            if (l >= 2 && l <= P.k - 2 && cnt > 0 && cnt <= kUnitItems) {
+            if (l == 1 && cnt > 0 && 2 * cnt <= kUnitItems) {
+              for (int t = 0; t < cnt; ++t) {
+                W.er[t] = u.items[2 * t];
+                W.ec[t] = u.items[2 * t + 1];
+              }
+            } else if (l >= 2 && l <= P.k - 2 && cnt > 0 && cnt <= kUnitItems) {
               for (int j = 0; j < l; ++j) W.phi[j] = u.phi[j];
               int32_t *mb = buf(l);
               for (int t = 0; t < cnt; ++t) mb[t] = u.items[t];
@@ -548,15 +576,15 @@ struct Engine {
     return l;
   }
 
-  // Busy warp: when some warp is hungry, move up to kUnitItems of the
-  // shallowest remaining candidates into the global ring.
+  // Busy warp: when some warp is hungry, move up to a unit's worth of the
+  // shallowest remaining items into the global ring.
   __device__ void maybe_donate(int level) {
     int hungry = 0;
     if (lane == 0) hungry = *(volatile int32_t *)&ctl->hungry;
     hungry = __shfl_sync(kFull, hungry, 0);
     if (hungry <= 0) return;
     if (lane == 0) {
-      int l = 2;
+      int l = 1;
       for (; l <= level; ++l) {
         const unsigned long long w = *(volatile unsigned long long *)&W.word[l];
         if ((int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu) >= 2) break;
@@ -564,13 +592,15 @@ struct Engine {
       if (l <= level) {
         const long long pos = queue_reserve();
         if (pos >= 0) {
+          const int maxtake = l == 1 ? kUnitItems / 2 : kUnitItems;
           int cnt = 0, from = 0;
           unsigned long long w = *(volatile unsigned long long *)&W.word[l];
           for (int t = 0; t < kCasLimit; ++t) {
             const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
             if (n - it < 2) break;
-            const int take = min((n - it) / 2, kUnitItems);
-            const unsigned long long old = atomicCAS(&W.word[l], w, (w & ~0xffffull) | (unsigned long long)(n - take));
+            const int take = min((n - it) / 2, maxtake);
+            const unsigned long long old =
+                atomicCAS(&W.word[l], w, (w & ~0xffffull) | (unsigned long long)(n - take));
             if (old == w) {
               cnt = take;
               from = n - take;
@@ -578,7 +608,7 @@ struct Engine {
             }
             w = old;
           }
-          queue_publish((unsigned long long)pos, l, buf(l) + from, cnt);
+          queue_publish((unsigned long long)pos, l, from, cnt);
           if (cnt) atomicAdd(&ctl->splits, 1ull);
         }
       }
@@ -586,30 +616,42 @@ struct Engine {
     __syncwarp();
   }
 
+  __device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+  }
+
   // ---- main loop ------------------------------------------------------------
+  // level 1 iterates edge pairs, 2..k-2 iterate buffered candidates, the last
+  // vertex k-1 is counted in place.  `base` is the shallowest level this warp
+  // owns: below it the warp acquires new work (an edge chunk, a steal from
+  // its CTA, or a unit from the global ring).
   __device__ void run(int nwarps, int me) {
     const int k = P.k;
-    int level = 1, base = 1;
+    int level = 0, base = 1;
     bool edges_left = true;
-    bool busy = true;   // counted in ctl->pending
-    bool hungry = false;  // counted in ctl->hungry
+    bool busy = true;     // counted in ctl->pending (warps that hold work)
+    bool hungry = false;  // counted in ctl->hungry (warps polling for work)
     unsigned claims = 0;
     if (lane == 0) {
-      W.en = W.eit = 0;
       for (int l = 0; l < kStoredMax; ++l) W.word[l] = 0;
       for (int l = 0; l < kMaxK; ++l) W.h[l].complete = 0;
+      if (cfg.steal) atomicAdd(&ctl->pending, 1);
     }
     __syncwarp();
     for (;;) {
       if (level < base) {
-        // ---- acquire new work: edges, then a local steal, then the ring ----
+        // ---- acquire new work ----
         level = 0;
         if (edges_left) {
           if (fetch_edges()) level = base = 1;
           else edges_left = false;
         }
         if (!level && cfg.steal) {
-          for (int polls = 0;; ++polls) {
+          const unsigned long long t0 = now_ns();
+          unsigned nap = 64;
+          for (;;) {
             int l = steal_local(nwarps, me);
             if (!l) l = queue_pop();
             if (l) {
@@ -628,12 +670,18 @@ struct Engine {
               const unsigned long long h = *(volatile unsigned long long *)&qh->head;
               const unsigned long long t = *(volatile unsigned long long *)&qh->tail;
               done = pend <= 0 && h == t;
+              // bounded wait: a warp idle for longer than the limit reports a
+              // timeout instead of spinning on (no work is lost: the busy
+              // warps drain the ring before they retire)
+              if (!done && now_ns() - t0 > (unsigned long long)cfg.idle_ms * 1000000ull) {
+                raise_error(ctl, TDFS_ERR_TIMEOUT);
+                done = 1;
+              }
             }
             done = __shfl_sync(kFull, done, 0);
-            // retiring early is safe: every unit is pushed by a busy warp,
-            // which drains the ring itself before it retires
-            if (done || polls >= cfg.poll_limit) break;
-            __nanosleep(polls < 64 ? 256 : 2048);
+            if (done) break;
+            __nanosleep(nap);
+            nap = min(nap * 2, 4096u);
           }
           if (level && lane == 0) {
             if (!busy) atomicAdd(&ctl->pending, 1);
@@ -647,38 +695,22 @@ struct Engine {
         if (!level) break;
         continue;
       }
-      if (level == 1) {
-        if (W.eit >= W.en) {
-          level = 0;  // chunk spent: acquire more
-          base = 1;
-          continue;
-        }
-        const int t = W.eit;
-        const int32_t r = W.er[t], c = W.ec[t];
-        __syncwarp();
-        if (lane == 0) {
-          W.eit = t + 1;
-          W.phi[0] = r;
-          W.phi[1] = c;
-        }
-        __syncwarp();
-        if (k == 3) {
-          count += count_last(2);
-        } else {
-          setup(2, true);
-          produce(2);
-          level = 2;
-        }
-        continue;
-      }
-      // stored level 2 <= level <= k-2
       const int32_t idx = claim(level);
       if (idx >= 0) {
-        const int32_t x = buf(level)[idx];
+        if (level == 1) {
+          const int32_t r = W.er[idx], c = W.ec[idx];
+          __syncwarp();
+          if (lane == 0) {
+            W.phi[0] = r;
+            W.phi[1] = c;
+          }
+        } else {
+          const int32_t x = buf(level)[idx];
+          __syncwarp();
+          if (lane == 0) W.phi[level] = x;
+        }
         __syncwarp();
-        if (lane == 0) W.phi[level] = x;
-        __syncwarp();
-        if (cfg.steal && ((++claims & 15u) == 0)) maybe_donate(level);
+        if (cfg.steal && ((++claims & 7u) == 0)) maybe_donate(level);
         if (level + 1 == k - 1) {
           count += count_last(k - 1);
         } else {
@@ -688,7 +720,7 @@ struct Engine {
         }
         continue;
       }
-      if (W.h[level].spos < W.h[level].send) {
+      if (level >= 2 && W.h[level].spos < W.h[level].send) {
         produce(level);
         continue;
       }
@@ -729,7 +761,7 @@ __global__ void init_kernel(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t 
     ctl->steals = 0;
     ctl->splits = 0;
     ctl->error = 0;
-    ctl->pending = total_warps;
+    ctl->pending = 0;  // warps add themselves when they start
     ctl->hungry = 0;
     qh->head = 0;
     qh->tail = 0;
@@ -744,6 +776,21 @@ size_t warp_smem_bytes(int k, int cap, int window) {
   const size_t hdr = (sizeof(WarpSmem) + 15) & ~(size_t)15;
   const int stored = k > 3 ? k - 3 : 0;
   return hdr + sizeof(int32_t) * ((size_t)window + (size_t)stored * cap);
+}
+
+int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem) {
+  int n = 0;
+  cudaError_t e;
+  if (labeled) {
+    e = cudaFuncSetAttribute(match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, match_kernel<true>, warps_per_block * 32, smem);
+  } else {
+    e = cudaFuncSetAttribute(match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, match_kernel<false>, warps_per_block * 32, smem);
+  }
+  return e == cudaSuccess ? n : -1;
 }
 
 void init_launch(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin, cudaStream_t stream) {

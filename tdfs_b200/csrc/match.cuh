@@ -49,7 +49,7 @@ struct KernelCfg {
   int32_t warp_bytes;   // shared memory per warp
   int32_t steal;        // 1: stealing + donation on
   int32_t window;       // merge window in ints (multiple of 128) or 0 = off
-  int32_t poll_limit;   // idle polls before a warp retires
+  int32_t idle_ms;      // bounded idle wait before a warp reports a timeout
   int32_t pad_;
 };
 
@@ -61,6 +61,10 @@ size_t warp_smem_bytes(int k, int cap, int window);
 // by init_launch on the same stream.
 int launch_match(const DevPlan &plan, const DevGraph &g, RunCtl *ctl, SplitUnit *units, QueueHdr *qh,
                  const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream);
+// CTAs of the match kernel that fit on one SM at once (registers, shared
+// memory, threads); -1 on a CUDA error.  The persistent grid must not exceed
+// this times the SM count: idle warps wait for busy ones.
+int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem);
 void init_launch(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin, cudaStream_t stream);
 
 }  // namespace tdfs

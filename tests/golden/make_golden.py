@@ -123,7 +123,11 @@ def make_ref_counts():
             for labeled in (False, True):
                 exe = os.path.join(REFBIN, "lb.out" if labeled else "ulb.out")
                 r = subprocess.run([exe, prefix, path], capture_output=True, text=True, timeout=600)
-                last = [l for l in r.stdout.splitlines() if l.count("\t") == 2][-1]
+                lines = [l for l in r.stdout.splitlines() if l.count("\t") == 2]
+                if r.returncode != 0 or not lines:
+                    raise RuntimeError(f"{exe} {pname}: rc={r.returncode}\nstdout tail: {r.stdout[-600:]}\n"
+                                       f"stderr: {r.stderr[-600:]}")
+                last = lines[-1]
                 _, ms, cnt = last.split("\t")
                 out.append({"graph": gname, "pattern": pname, "text": text, "labeled": labeled,
                             "count": int(cnt), "ms": float(ms)})
