@@ -25,9 +25,11 @@ static_assert(sizeof(SplitUnit) % 16 == 0, "unit alignment");
 
 // Bounded MPMC ring (per-slot sequence numbers) header, followed in memory
 // by kQueueCap sequence words and kQueueCap units.
-struct QueueHdr {
+struct alignas(128) QueueHdr {
   unsigned long long head;
+  char pad0_[120];
   unsigned long long tail;
+  char pad1_[120];
   unsigned long long seq[kQueueCap];
 };
 

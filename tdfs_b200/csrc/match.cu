@@ -113,17 +113,18 @@ __device__ __forceinline__ bool test_lists(bool ok, int32_t x, const LevelHdr &H
     int32_t p = 0;
     const bool searched = ok;
     if ((H.merge_mask >> m & 1) && __any_sync(kFull, ok)) {
-      // stage L[cur .. cur + window) (16-byte aligned) in shared memory
+      // stage L[cur .. cur + window) in shared memory with 16-byte loads from
+      // the aligned offset below cur, but no further than the list's end
       const int64_t off = (int64_t)(L - colidx) + cur[m];
       const int64_t a0 = off & ~(int64_t)3;
-      const int4 *gsrc = reinterpret_cast<const int4 *>(colidx + a0);
-      for (int t = lane; t < (window >> 2); t += 32) reinterpret_cast<int4 *>(win)[t] = __ldg(gsrc + t);
-      __syncwarp();
-      // window covers global offsets [a0, a0 + window) intersected with the list
-      const int32_t first = (int32_t)(off - a0);                      // index of cur in win
       const int64_t lend = (int64_t)(L - colidx) + len;
       const int64_t wend = lend - a0;
       const int32_t last = (int32_t)(wend < (int64_t)window ? wend : (int64_t)window);  // exclusive
+      const int4 *gsrc = reinterpret_cast<const int4 *>(colidx + a0);
+      const int nvec = (max(last, 0) + 3) >> 2;
+      for (int t = lane; t < nvec; t += 32) reinterpret_cast<int4 *>(win)[t] = __ldg(gsrc + t);
+      __syncwarp();
+      const int32_t first = (int32_t)(off - a0);  // index of cur in win
       if (ok) {
         if (first < last && x <= win[last - 1]) {
           const int32_t q = lower_bound(win, first, last, x);
@@ -650,10 +651,20 @@ struct Engine {
         }
         if (!level && cfg.steal) {
           const unsigned long long t0 = now_ns();
-          unsigned nap = 64;
+          unsigned nap = 256;
           for (;;) {
             int l = steal_local(nwarps, me);
-            if (!l) l = queue_pop();
+            // one look at the ring: pop only when it holds units; retire when
+            // it is empty and no warp holds work
+            int state = 0;  // 0 wait, 1 ring non-empty, 2 done
+            if (!l && lane == 0) {
+              const unsigned long long h = *(volatile unsigned long long *)&qh->head;
+              const unsigned long long t = *(volatile unsigned long long *)&qh->tail;
+              if (h < t) state = 1;
+              else if (*(volatile int32_t *)&ctl->pending <= (busy ? 1 : 0)) state = 2;
+            }
+            state = __shfl_sync(kFull, state, 0);
+            if (!l && state == 1) l = queue_pop();
             if (l) {
               level = base = l;
               break;
@@ -664,24 +675,18 @@ struct Engine {
             }
             busy = false;
             hungry = true;
-            int done = 0;
-            if (lane == 0) {
-              const int pend = *(volatile int32_t *)&ctl->pending;
-              const unsigned long long h = *(volatile unsigned long long *)&qh->head;
-              const unsigned long long t = *(volatile unsigned long long *)&qh->tail;
-              done = pend <= 0 && h == t;
-              // bounded wait: a warp idle for longer than the limit reports a
-              // timeout instead of spinning on (no work is lost: the busy
-              // warps drain the ring before they retire)
-              if (!done && now_ns() - t0 > (unsigned long long)cfg.idle_ms * 1000000ull) {
-                raise_error(ctl, TDFS_ERR_TIMEOUT);
-                done = 1;
-              }
+            int done = state == 2;
+            // bounded wait: a warp idle for longer than the limit reports a
+            // timeout instead of spinning on (no work is lost: the busy warps
+            // drain the ring before they retire)
+            if (!done && lane == 0 && now_ns() - t0 > (unsigned long long)cfg.idle_ms * 1000000ull) {
+              raise_error(ctl, TDFS_ERR_TIMEOUT);
+              done = 1;
             }
             done = __shfl_sync(kFull, done, 0);
             if (done) break;
             __nanosleep(nap);
-            nap = min(nap * 2, 4096u);
+            nap = min(nap * 2, 8192u);
           }
           if (level && lane == 0) {
             if (!busy) atomicAdd(&ctl->pending, 1);
