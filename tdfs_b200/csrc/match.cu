@@ -98,13 +98,36 @@ __device__ __forceinline__ bool pass_filter(int32_t x, const LevelHdr &H, int i,
   return true;
 }
 
+// Stage L[cur .. cur + window) of membership list m in shared memory with
+// 16-byte loads from the aligned offset below cur, no further than the list's
+// end.  Returns the staged extent; the caller syncs the warp before reading.
+struct Window {
+  int32_t first;  // index of the cursor position inside win
+  int32_t last;   // exclusive end of valid entries in win
+};
+
+__device__ __forceinline__ Window stage_window(const int32_t *L, int32_t len, int32_t cur, int32_t *win,
+                                               int window, const int32_t *colidx) {
+  const int lane = lane_id();
+  const int64_t off = (int64_t)(L - colidx) + cur;
+  const int64_t a0 = off & ~(int64_t)3;
+  const int64_t wend = (int64_t)(L - colidx) + len - a0;
+  Window w;
+  w.last = (int32_t)(wend < (int64_t)window ? wend : (int64_t)window);
+  w.first = (int32_t)(off - a0);
+  const int4 *gsrc = reinterpret_cast<const int4 *>(colidx + a0);
+  const int nvec = (max(w.last, 0) + 3) >> 2;
+  for (int t = lane; t < nvec; t += 32) reinterpret_cast<int4 *>(win)[t] = __ldg(gsrc + t);
+  return w;
+}
+
 // Membership of each lane's x in the level's other lists.  `ok` lanes are
-// tested; cursors advance monotonically (the source is sorted).  `win` is the
-// warp's staging area for the merge path.
+// tested; cursors advance monotonically (the source is sorted).  List 0's
+// window may already be staged (`w0`, issued together with the source load
+// so the two memory round trips overlap); `win` is the warp's staging area.
 __device__ __forceinline__ bool test_lists(bool ok, int32_t x, const LevelHdr &H,
                                            int32_t (&cur)[kMaxLists], int32_t *win, int window,
-                                           const int32_t *colidx) {
-  const int lane = lane_id();
+                                           const int32_t *colidx, bool staged0, Window w0) {
 #pragma unroll
   for (int m = 0; m < kMaxLists; ++m) {
     if (m >= H.nm) break;
@@ -112,26 +135,17 @@ __device__ __forceinline__ bool test_lists(bool ok, int32_t x, const LevelHdr &H
     const int32_t len = H.mlen[m];
     int32_t p = 0;
     const bool searched = ok;
-    if ((H.merge_mask >> m & 1) && __any_sync(kFull, ok)) {
-      // stage L[cur .. cur + window) in shared memory with 16-byte loads from
-      // the aligned offset below cur, but no further than the list's end
-      const int64_t off = (int64_t)(L - colidx) + cur[m];
-      const int64_t a0 = off & ~(int64_t)3;
-      const int64_t lend = (int64_t)(L - colidx) + len;
-      const int64_t wend = lend - a0;
-      const int32_t last = (int32_t)(wend < (int64_t)window ? wend : (int64_t)window);  // exclusive
-      const int4 *gsrc = reinterpret_cast<const int4 *>(colidx + a0);
-      const int nvec = (max(last, 0) + 3) >> 2;
-      for (int t = lane; t < nvec; t += 32) reinterpret_cast<int4 *>(win)[t] = __ldg(gsrc + t);
+    const bool merge = H.merge_mask >> m & 1;
+    if (merge && ((m == 0 && staged0) || __any_sync(kFull, ok))) {
+      const Window w = (m == 0 && staged0) ? w0 : stage_window(L, len, cur[m], win, window, colidx);
       __syncwarp();
-      const int32_t first = (int32_t)(off - a0);  // index of cur in win
       if (ok) {
-        if (first < last && x <= win[last - 1]) {
-          const int32_t q = lower_bound(win, first, last, x);
-          p = cur[m] + (q - first);
+        if (w.first < w.last && x <= win[w.last - 1]) {
+          const int32_t q = lower_bound(win, w.first, w.last, x);
+          p = cur[m] + (q - w.first);
           ok = win[q] == x;
         } else {
-          const int32_t from = cur[m] + max(0, last - first);
+          const int32_t from = cur[m] + max(0, w.last - w.first);
           p = lower_bound(L, from, len, x);
           ok = p < len && L[p] == x;
         }
@@ -241,8 +255,11 @@ struct Engine {
         else neq[nneq++] = v;
       }
     }
+    // skip the prefix <= lo by a 32-ary search; a short source is cheaper to
+    // filter in the scan, except when the closed-form count needs the bound
     int32_t spos = 0;
-    if (!LAB && lo >= 0 && slen > 0) spos = warp_upper_bound(src, 0, slen, lo);
+    const bool closed = !LAB && nm == 0 && hi == INT_MAX && i == P.k - 1;
+    if (!LAB && lo >= 0 && slen > 0 && (slen > 64 || closed)) spos = warp_upper_bound(src, 0, slen, lo);
     // merge (staged window) or per-lane search, per list, by degree ratio
     uint32_t mm = 0;
     if (cfg.window > 0 && myslot >= 0 && (int64_t)mylen <= 4ll * max(1, slen - spos)) mm = 1u << myslot;
@@ -279,8 +296,11 @@ struct Engine {
       const int32_t idx = spos + lane;
       const bool valid = idx < send;
       const int32_t x = valid ? src[idx] : 0;
+      const bool st0 = H.nm > 0 && (H.merge_mask & 1u);
+      Window w0 = {0, 0};
+      if (st0) w0 = stage_window(H.mlist[0], H.mlen[0], cur[0], win, cfg.window, G.colidx);
       bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
-      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx);
+      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx, st0, w0);
       const unsigned mask = __ballot_sync(kFull, ok);
       if (ok) out[n + __popc(mask & lanemask_lt())] = x;
       n += __popc(mask);
@@ -334,8 +354,11 @@ struct Engine {
       const int32_t idx = spos + lane;
       const bool valid = idx < send;
       const int32_t x = valid ? src[idx] : 0;
+      const bool st0 = H.nm > 0 && (H.merge_mask & 1u);
+      Window w0 = {0, 0};
+      if (st0) w0 = stage_window(H.mlist[0], H.mlen[0], cur[0], win, cfg.window, G.colidx);
       bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
-      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx);
+      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx, st0, w0);
       c += __popc(__ballot_sync(kFull, ok));
     }
     return c;
