@@ -151,12 +151,19 @@ def test_reference_failure_independent_recount(T):
     lines = r["text"].splitlines()
     k = sum(1 for l in lines if l.startswith("v"))
     edges = [tuple(map(int, l.split()[1:3])) for l in lines if l.startswith("e")]
-    back = {i: [a if b == i else b for a, b in edges if (a == i and b < i) or (b == i and a < i)] for i in range(k)}
+    nbr = {i: {b if a == i else a for a, b in edges if i in (a, b)} for i in range(k)}
+    # the count does not depend on the enumeration order: place the most
+    # constrained vertex next (most placed neighbours, then highest degree)
+    order = [max(range(k), key=lambda v: len(nbr[v]))]
+    while len(order) < k:
+        order.append(max((v for v in range(k) if v not in order),
+                         key=lambda v: (len(nbr[v] & set(order)), len(nbr[v]))))
+    back = [[order.index(u) for u in nbr[order[i]] if order.index(u) < i] for i in range(k)]
 
     def rec(i, phi):
-        if i == k:
-            return 1
         cand = set.intersection(*[adj[phi[j]] for j in back[i]])
+        if i == k - 1:  # the last vertex: count, do not recurse
+            return len(cand.difference(phi))
         return sum(rec(i + 1, phi + [x]) for x in cand if x not in phi)
 
     total = sum(rec(2, [u, v]) for u in range(g.n) for v in adj[u])
