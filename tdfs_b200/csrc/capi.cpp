@@ -59,7 +59,7 @@ int cuda_err(cudaError_t e, const char *what) {
 }
 
 // Choose the launch shape: a persistent grid of (resident CTAs per SM) x SMs.
-int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, LaunchShape *out) {
+int plan_launch(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out) {
   // device properties are queried once per device (the query costs ~ms)
   static cudaDeviceProp props[64];
   static bool have[64] = {};
@@ -74,7 +74,7 @@ int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, La
   std::memset(&s, 0, sizeof s);
   s.warps_per_block = o.warps_per_block > 0 ? o.warps_per_block : 8;
   if (s.warps_per_block > 8) return fail(TDFS_ERR_ARG, "warps_per_block must be <= 8");
-  int cap = o.chunk_cap > 0 ? o.chunk_cap : (p.k >= 6 ? 256 : 512);
+  int cap = o.chunk_cap > 0 ? o.chunk_cap : (kmax >= 6 ? 256 : 512);
   cap = (cap + 31) & ~31;
   if (cap < 64 || cap > 8192) return fail(TDFS_ERR_ARG, "chunk_cap must lie in [64, 8192]");
   int window = o.merge_window == 0 ? 128 : (o.merge_window < 0 ? 0 : o.merge_window);
@@ -82,52 +82,89 @@ int plan_launch(const tdfs_graph *g, const DevPlan &p, const tdfs_options &o, La
   KernelCfg &c = s.cfg;
   c.cap = cap;
   c.window = window;
-  c.warp_bytes = (int)((warp_smem_bytes(p.k, cap, window) + 15) & ~(size_t)15);
+  c.warp_bytes = (int)((warp_smem_bytes(kmax, cap, window) + 15) & ~(size_t)15);
   c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
   c.idle_ms = 30000;
-  c.e_begin = std::max<int64_t>(0, o.edge_begin);
-  c.e_end = (o.edge_end < 0 || o.edge_end > g->nedges) ? g->nedges : o.edge_end;
-  c.stride = o.edge_stride > 0 ? o.edge_stride : 1;
-  c.phase = o.edge_phase;
-  if (c.phase < 0 || c.phase >= c.stride) return fail(TDFS_ERR_ARG, "edge_phase must lie in [0, edge_stride)");
   const size_t smem = (size_t)c.warp_bytes * s.warps_per_block;
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
                 smem, (size_t)prop.sharedMemPerBlockOptin);
-  const int fit = resident_blocks_per_sm(p.labeled != 0, s.warps_per_block, smem);
+  const int fit = resident_blocks_per_sm(labeled, s.warps_per_block, smem);
   if (fit < 0) return fail(TDFS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
   if (fit == 0) return fail(TDFS_ERR_CAPACITY, "the match kernel does not fit on an SM with this shape");
   // a persistent grid: every CTA resident at once (idle warps wait on busy ones)
-  int per_sm = o.blocks_per_sm > 0 ? std::min(o.blocks_per_sm, fit) : fit;
+  const int per_sm = o.blocks_per_sm > 0 ? std::min(o.blocks_per_sm, fit) : fit;
   s.blocks = prop.multiProcessorCount * per_sm;
   *out = s;
   return TDFS_OK;
 }
 
-// Launch the counting kernel for one plan on the graph's workspace and
-// return the raw (pre-multiplier) count.
-int run_one(tdfs_graph *g, const DevPlan &p, const tdfs_options &o, unsigned long long *raw, float *ms) {
-  if (p.labeled && !g->labeled) return fail(TDFS_ERR_ARG, "labeled pattern on a graph opened without labels");
+// Level-0 tickets of an edge range dealt round-robin: ticket t covers the
+// chunk of 32 edges starting at e_begin + (t * stride + phase) * 32.
+int64_t ticket_count(int64_t b, int64_t e, int stride, int phase) {
+  const int64_t chunks = (e - b + kEdgeChunk - 1) / kEdgeChunk;
+  if (chunks <= phase) return 0;
+  return (chunks - phase + stride - 1) / stride;
+}
+
+// One launch over n plans of the same mode: slot i counts plans[i] on the
+// option's edge range; raw[i] receives the count before the |Aut| multiplier.
+int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_options &o, unsigned long long *raw,
+              float *ms) {
+  if (n <= 0) return TDFS_OK;
+  if (n > kMaxSlots) return fail(TDFS_ERR_CAPACITY, "at most %d plans per launch", kMaxSlots);
+  const bool labeled = plans[0]->labeled != 0;
+  int kmax = 3;
+  for (int i = 0; i < n; ++i) {
+    if ((plans[i]->labeled != 0) != labeled) return fail(TDFS_ERR_ARG, "a launch mixes labeled and unlabeled plans");
+    kmax = std::max(kmax, (int)plans[i]->k);
+  }
+  if (labeled && !g->labeled) return fail(TDFS_ERR_ARG, "labeled pattern on a graph opened without labels");
   cudaError_t e = cudaSetDevice(g->device);
   if (e != cudaSuccess) return cuda_err(e, "cudaSetDevice");
   LaunchShape s;
-  int rc = plan_launch(g, p, o, &s);
+  int rc = plan_launch(g, kmax, labeled, o, &s);
   if (rc) return rc;
+  const int64_t eb = std::max<int64_t>(0, o.edge_begin);
+  const int64_t ee = (o.edge_end < 0 || o.edge_end > g->nedges) ? g->nedges : o.edge_end;
+  const int stride = o.edge_stride > 0 ? o.edge_stride : 1;
+  if (o.edge_phase < 0 || o.edge_phase >= stride) return fail(TDFS_ERR_ARG, "edge_phase must lie in [0, edge_stride)");
+  SlotTable *h = g->htab;
+  std::memset(&h->ctl, 0, sizeof h->ctl);
+  h->ctl.admitted = (unsigned long long)n;
+  h->ctl.shutdown = 1;
+  for (int i = 0; i < n; ++i) {
+    SlotInfo &in = h->info[i];
+    in.e_begin = eb;
+    in.e_end = std::max(eb, ee);
+    in.stride = stride;
+    in.phase = o.edge_phase;
+    in.ntickets = ticket_count(in.e_begin, in.e_end, stride, o.edge_phase);
+    std::memset(&h->hot[i], 0, sizeof h->hot[i]);
+    h->hot[i].state = in.ntickets > 0 ? kSlotActive : kSlotDone;  // an empty range is done at once
+    if (in.ntickets == 0) ++h->ctl.completed;
+    h->plan[i] = *plans[i];
+  }
   cudaStream_t st = static_cast<cudaStream_t>(o.stream);
-  QueueHdr *qh = queue_hdr(g);
-  const int total_warps = s.blocks * s.warps_per_block;
+  SlotTable *d = g->tab;
+  e = cudaMemcpyAsync(&d->ctl, &h->ctl, sizeof h->ctl, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d->hot, h->hot, sizeof(SlotHot) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d->info, h->info, sizeof(SlotInfo) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d->plan, h->plan, sizeof(DevPlan) * n, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_err(e, "slot table upload");
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   if (ms) {
     cudaEventCreate(&ev0);
     cudaEventCreate(&ev1);
   }
-  init_launch(g->ctl, qh, total_warps, s.cfg.e_begin, st);
+  init_launch(g->ctl, queue_hdr(g), st);
   if (ms) cudaEventRecord(ev0, st);
-  rc = launch_match(p, graph_view(g), g->ctl, g->queue, qh, s.cfg, s.blocks, s.warps_per_block, st);
+  rc = launch_match(labeled, graph_view(g), g->ctl, d, g->queue, queue_hdr(g), s.cfg, s.blocks, s.warps_per_block, st);
   if (ms) cudaEventRecord(ev1, st);
-  RunCtl h;
+  RunCtl hc;
   if (!rc) {
-    e = cudaMemcpyAsync(&h, g->ctl, sizeof h, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(h->hot, d->hot, sizeof(SlotHot) * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, g->ctl, sizeof hc, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_err(e, "match kernel");
   }
@@ -138,9 +175,12 @@ int run_one(tdfs_graph *g, const DevPlan &p, const tdfs_options &o, unsigned lon
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (rc) return rc;
-  if (h.error == TDFS_ERR_TIMEOUT) return fail(TDFS_ERR_TIMEOUT, "a bounded device wait ran out");
-  if (h.error) return fail(h.error, "device error %d", h.error);
-  *raw = h.count;
+  if (hc.error == TDFS_ERR_TIMEOUT) return fail(TDFS_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (hc.error) return fail(hc.error, "device error %d", hc.error);
+  for (int i = 0; i < n; ++i) {
+    if (h->hot[i].state != kSlotDone) return fail(TDFS_ERR_TIMEOUT, "slot %d did not complete", i);
+    raw[i] = h->hot[i].count;
+  }
   return TDFS_OK;
 }
 
@@ -249,7 +289,8 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
   tdfs_options o;
   if (opt) o = *opt; else tdfs_options_default(&o);
   unsigned long long raw = 0;
-  int rc = run_one(g, p->dev, o, &raw, kernel_ms);
+  const DevPlan *dp = &p->dev;
+  int rc = run_batch(g, &dp, 1, o, &raw, kernel_ms);
   if (rc) return rc;
   // cu_test.cu:100-105: the unlabeled total is multiplied by |Aut|
   *count = (uint64_t)(raw * (unsigned long long)p->dev.multiplicity);
@@ -259,12 +300,30 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
 int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *opt,
                      uint64_t *counts, float *kernel_ms) {
   if (!g || (!plans && nplans) || (!counts && nplans) || nplans < 0) return fail(TDFS_ERR_ARG, "bad arguments");
+  tdfs_options o;
+  if (opt) o = *opt; else tdfs_options_default(&o);
   float total = 0.f;
-  for (int i = 0; i < nplans; ++i) {
-    float ms = 0.f;
-    int rc = tdfs_count(g, plans[i], opt, &counts[i], kernel_ms ? &ms : nullptr);
-    if (rc) return rc;
-    total += ms;
+  // one launch per mode (a launch runs either the labeled or the unlabeled kernel)
+  for (int mode = 0; mode < 2; ++mode) {
+    std::vector<const DevPlan *> dp;
+    std::vector<int> idx;
+    for (int i = 0; i < nplans; ++i) {
+      if (!plans[i]) return fail(TDFS_ERR_ARG, "null plan %d", i);
+      if ((plans[i]->dev.labeled != 0) == (mode == 1)) {
+        dp.push_back(&plans[i]->dev);
+        idx.push_back(i);
+      }
+    }
+    for (size_t b = 0; b < dp.size(); b += kMaxSlots) {
+      const int n = (int)std::min<size_t>(kMaxSlots, dp.size() - b);
+      std::vector<unsigned long long> raw(n);
+      float ms = 0.f;
+      int rc = run_batch(g, dp.data() + b, n, o, raw.data(), kernel_ms ? &ms : nullptr);
+      if (rc) return rc;
+      total += ms;
+      for (int j = 0; j < n; ++j)
+        counts[idx[b + j]] = (uint64_t)(raw[j] * (unsigned long long)dp[b + j]->multiplicity);
+    }
   }
   if (kernel_ms) *kernel_ms = total;
   return TDFS_OK;

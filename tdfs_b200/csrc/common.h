@@ -53,17 +53,12 @@ struct DevGraph {
 // sit on their own 128-byte lines so ticket atomics, idle polling and the
 // final count do not serialise on one L2 line.
 struct alignas(128) RunCtl {
-  unsigned long long edge_next;  // level-0 chunk ticket counter
-  char pad0_[120];
-  int32_t pending;               // warps holding work
-  char pad1_[124];
   int32_t hungry;                // warps idle and looking for work
-  char pad2_[124];
-  unsigned long long count;      // raw (pre-multiplier) total
+  char pad0_[124];
   unsigned long long steals;     // diagnostics: intra-block steals
   unsigned long long splits;     // diagnostics: units through the global queue
   int32_t error;                 // TDFS_ERR_* raised by the kernel
-  char pad3_[100];
+  char pad1_[108];
 };
 
 // Error reporting shared by the C ABI implementation files.

@@ -84,6 +84,10 @@ void release(tdfs_graph *g) {
   cudaFree(g->label);
   cudaFree(g->ctl);
   cudaFree(g->queue);
+  cudaFree(g->tab);
+  if (g->htab) cudaFreeHost(g->htab);
+  g->tab = nullptr;
+  g->htab = nullptr;
   g->rowptr = nullptr;
   g->colidx = nullptr;
   g->src = nullptr;
@@ -118,6 +122,8 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   CK(cudaMalloc(&g->maxnd, sizeof(int32_t) * (n ? n : 1)));
   CK(cudaMalloc(&g->ctl, sizeof(RunCtl)));
   CK(cudaMalloc(&g->queue, sizeof(SplitUnit) * kQueueCap + sizeof(QueueHdr)));
+  CK(cudaMalloc(&g->tab, sizeof(SlotTable)));
+  CK(cudaMallocHost(&g->htab, sizeof(SlotTable)));
   CK(cudaMemcpy(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(g->colidx, colidx, sizeof(int32_t) * nedges, cudaMemcpyHostToDevice));
   CK(cudaMemset(g->colidx + nedges, 0x7f, sizeof(int32_t) * kColPad));

@@ -19,7 +19,8 @@ struct SplitUnit {
   int32_t nitems;
   int32_t phi[kMaxK];
   int32_t items[kUnitItems];
-  int32_t pad_[7];
+  int32_t slot;     // query the subtree belongs to
+  int32_t pad_[6];
 };
 static_assert(sizeof(SplitUnit) % 16 == 0, "unit alignment");
 
@@ -31,6 +32,53 @@ struct alignas(128) QueueHdr {
   unsigned long long tail;
   char pad1_[120];
   unsigned long long seq[kQueueCap];
+};
+
+// ---- query slots ----------------------------------------------------------
+// Every launch works through a table of query slots: one slot per pattern of
+// a batched launch, or one per admitted query of the serving loop.  Slots are
+// filled by the host before the kernel may see them (`admitted`) and are never
+// reused within one launch, so a warp holding a stale slot index can only
+// touch a finished slot, never a recycled one.
+constexpr int kMaxSlots = 4096;
+
+enum : int32_t { kSlotEmpty = 0, kSlotActive = 1, kSlotDone = 2 };
+
+// Counters that warps update: one 128-byte line per slot.
+struct alignas(128) SlotHot {
+  unsigned long long ticket;  // next level-0 chunk ticket
+  unsigned long long count;   // raw count (before the |Aut| multiplier)
+  int32_t holders;            // warps holding this query's work + its queued units
+  int32_t state;              // kSlotActive -> kSlotDone (by the completing warp)
+  unsigned long long t_first; // globaltimer when the first ticket was taken
+  unsigned long long t_done;  // globaltimer at completion
+};
+
+// Written by the host at admission, read-only for the kernel.
+struct SlotInfo {
+  int64_t e_begin;   // level-0 edge range and round-robin dealing
+  int64_t e_end;
+  int64_t ntickets;  // tickets of this slot
+  int32_t stride, phase;
+};
+
+struct alignas(128) SlotCtl {
+  unsigned long long admitted;   // host: slots [0, admitted) are filled in
+  char pad0_[120];
+  unsigned long long completed;  // device: slots completed
+  char pad1_[120];
+  int32_t shutdown;              // host: 1 = no further admissions this launch
+  int32_t idle_exit_ms;          // serving: retire after this long with no work
+  char pad2_[120];
+  unsigned long long first_open; // device hint: slots below this have no tickets left
+  char pad3_[120];
+};
+
+struct SlotTable {
+  SlotCtl ctl;
+  SlotHot hot[kMaxSlots];
+  SlotInfo info[kMaxSlots];
+  DevPlan plan[kMaxSlots];
 };
 
 }  // namespace tdfs
@@ -48,6 +96,8 @@ struct tdfs_graph {
   uint8_t *label;
   tdfs::RunCtl *ctl;     // launch control block (one launch at a time per handle)
   tdfs::SplitUnit *queue; // split-unit ring: kQueueCap units then a QueueHdr
+  tdfs::SlotTable *tab;   // query slots of a launch
+  tdfs::SlotTable *htab;  // pinned host staging copy of the slot table
   size_t bytes;
 };
 

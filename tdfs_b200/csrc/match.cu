@@ -42,6 +42,9 @@ struct LevelHdr {
 
 struct alignas(16) WarpSmem {
   unsigned long long word[kStoredMax];  // per level 1..k-2: gen:32 | next:16 | end:16
+  DevPlan plan;                  // plan of the query this warp works on
+  int32_t slot;                  // its slot (-1: none)
+  int32_t pad0_[3];
   int32_t phi[kMaxK + 1];
   int32_t er[kEdgeChunk];        // level-1 items: edge pairs (phi(0), phi(1))
   int32_t ec[kEdgeChunk];
@@ -163,10 +166,11 @@ __device__ __forceinline__ bool test_lists(bool ok, int32_t x, const LevelHdr &H
 
 template <bool LAB>
 struct Engine {
-  const DevPlan &P;
+  const DevPlan &P;  // W.plan
   const DevGraph &G;
   const KernelCfg &cfg;
   RunCtl *ctl;
+  SlotTable *tab;
   SplitUnit *units;
   QueueHdr *qh;
   WarpSmem &W;
@@ -177,9 +181,9 @@ struct Engine {
   unsigned long long count = 0;
   int lane;
 
-  __device__ Engine(const DevPlan &p, const DevGraph &g, const KernelCfg &c, RunCtl *ct, SplitUnit *u,
-                    QueueHdr *q, WarpSmem &w, int32_t *b, int32_t *wn)
-      : P(p), G(g), cfg(c), ctl(ct), units(u), qh(q), W(w), bufs(b), win(wn), lane(lane_id()) {
+  __device__ Engine(const DevGraph &g, const KernelCfg &c, RunCtl *ct, SlotTable *tb, SplitUnit *u, QueueHdr *q,
+                    WarpSmem &w, int32_t *b, int32_t *wn)
+      : P(w.plan), G(g), cfg(c), ctl(ct), tab(tb), units(u), qh(q), W(w), bufs(b), win(wn), lane(lane_id()) {
     extern __shared__ __align__(16) unsigned char smem[];
     cta = smem;
     hdr_bytes = (sizeof(WarpSmem) + 15) & ~(size_t)15;
@@ -388,37 +392,125 @@ struct Engine {
     return __shfl_sync(kFull, r, 0);
   }
 
-  // Level-0 chunk: up to 32 directed edges, filtered as get_job
-  // (src/gpu_match.cu:531-556), published as this warp's level-1 items
-  // (pairs phi(0), phi(1)).  Returns false once the edge range is spent.
-  __device__ bool fetch_edges() {
+  // ---- query slots ----------------------------------------------------------
+
+  __device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+  }
+
+  // Copy slot s's plan into this warp's shared memory (all lanes).
+  __device__ void load_plan(int s) {
+    if (W.slot == s) return;
+    __syncwarp();
+    const int32_t *srcw = reinterpret_cast<const int32_t *>(&tab->plan[s]);
+    int32_t *dstw = reinterpret_cast<int32_t *>(&W.plan);
+    for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dstw[t] = srcw[t];
+    if (lane == 0) W.slot = s;
+    __syncwarp();
+  }
+
+  // Give up this warp's hold on slot s (lane 0).  Its count is added first;
+  // the warp that drops the last hold after the tickets ran out completes the
+  // slot, exactly once (CAS on the state).
+  __device__ void release_lane0(int s) {
+    SlotHot &h = tab->hot[s];
+    if (count) {
+      atomicAdd(&h.count, count);
+      count = 0;
+    }
+    __threadfence();
+    const int old = atomicSub(&h.holders, 1);
+    if (old == 1) {
+      const unsigned long long t = *(volatile unsigned long long *)&h.ticket;
+      if ((long long)t >= tab->info[s].ntickets && atomicCAS(&h.state, kSlotActive, kSlotDone) == kSlotActive) {
+        h.t_done = now_ns();
+        __threadfence();
+        atomicAdd(&tab->ctl.completed, 1ull);
+      }
+    }
+  }
+
+  // Level-0 chunk t of slot s: up to 32 directed edges, filtered as get_job
+  // (src/gpu_match.cu:531-556), published as level-1 items (pairs phi(0),
+  // phi(1)).  Returns false when no edge of the chunk passes the filter.
+  __device__ bool fetch_chunk(int s, long long t) {
+    const SlotInfo &in = tab->info[s];
+    const int64_t e0 = in.e_begin + (t * in.stride + in.phase) * (int64_t)kEdgeChunk;
+    const int64_t e = e0 + lane;
+    bool ok = e < in.e_end;
+    int32_t r = 0, c = 0;
+    if (ok) {
+      r = G.src[e];
+      c = G.colidx[e];
+      if (!LAB && P.orient && !(r < c)) ok = false;
+      if (LAB && ok && ((int32_t)G.label[r] != P.label[0] || (int32_t)G.label[c] != P.label[1])) ok = false;
+      if (ok && (deg(r) < P.deg[0] || deg(c) < P.deg[1] || G.maxnd[c] < P.deg[2])) ok = false;
+    }
+    const unsigned mask = __ballot_sync(kFull, ok);
+    if (ok) {
+      const int slot = __popc(mask & lanemask_lt());
+      W.er[slot] = r;
+      W.ec[slot] = c;
+    }
+    __syncwarp();
+    if (!mask) return false;
+    if (lane == 0) {
+      for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
+      publish(1, __popc(mask));
+    }
+    __syncwarp();
+    return true;
+  }
+
+  // Take level-0 tickets from open slots until a chunk yields edges.  On
+  // success this warp holds the slot; false when no slot has tickets left.
+  __device__ bool take_tickets() {
+    SlotCtl &C = tab->ctl;
     for (;;) {
-      unsigned long long t = 0;
-      if (lane == 0) t = atomicAdd(&ctl->edge_next, 1ull);
+      int s = -1;
+      long long t = 0;
+      if (lane == 0) {
+        const unsigned long long adm = *(volatile unsigned long long *)&C.admitted;
+        unsigned long long lo = *(volatile unsigned long long *)&C.first_open;
+        for (unsigned long long q = lo; q < adm && s < 0; ++q) {
+          SlotHot &h = tab->hot[q];
+          const long long nt = tab->info[q].ntickets;
+          if ((long long)*(volatile unsigned long long *)&h.ticket >= nt) {
+            if (q == lo) {  // advance the hint past exhausted slots
+              atomicMax(&C.first_open, q + 1);
+              lo = q + 1;
+            }
+            continue;
+          }
+          atomicAdd(&h.holders, 1);  // hold before taking: completion needs holders == 0
+          const unsigned long long tk = atomicAdd(&h.ticket, 1ull);
+          if ((long long)tk < nt) {
+            if (tk == 0) atomicCAS(&h.t_first, 0ull, now_ns());
+            s = (int)q;
+            t = (long long)tk;
+          } else {
+            release_lane0((int)q);  // nothing to flush: this warp holds no work
+          }
+        }
+      }
+      s = __shfl_sync(kFull, s, 0);
       t = __shfl_sync(kFull, t, 0);
-      const int64_t e0 = cfg.e_begin + ((int64_t)t * cfg.stride + cfg.phase) * kEdgeChunk;
-      if (e0 >= cfg.e_end) return false;
-      const int64_t e = e0 + lane;
-      bool ok = e < cfg.e_end;
-      int32_t r = 0, c = 0;
-      if (ok) {
-        r = G.src[e];
-        c = G.colidx[e];
-        if (!LAB && P.orient && !(r < c)) ok = false;
-        if (LAB && ok && ((int32_t)G.label[r] != P.label[0] || (int32_t)G.label[c] != P.label[1])) ok = false;
-        if (ok && (deg(r) < P.deg[0] || deg(c) < P.deg[1] || G.maxnd[c] < P.deg[2])) ok = false;
-      }
-      const unsigned mask = __ballot_sync(kFull, ok);
-      if (ok) {
-        const int slot = __popc(mask & lanemask_lt());
-        W.er[slot] = r;
-        W.ec[slot] = c;
-      }
-      __syncwarp();
-      if (mask) {
-        if (lane == 0) publish(1, __popc(mask));
-        __syncwarp();
-        return true;
+      if (s < 0) return false;
+      load_plan(s);
+      // keep taking tickets of this slot until a chunk yields edges
+      for (;;) {
+        if (fetch_chunk(s, t)) return true;
+        long long nt = 0;
+        if (lane == 0) {
+          const unsigned long long tk = atomicAdd(&tab->hot[s].ticket, 1ull);
+          nt = (long long)tk < tab->info[s].ntickets ? (long long)tk : -1;
+          if (nt < 0) release_lane0(s);
+        }
+        nt = __shfl_sync(kFull, nt, 0);
+        if (nt < 0) break;  // this slot is spent: look at the others
+        t = nt;
       }
     }
   }
@@ -441,7 +533,7 @@ struct Engine {
   }
 
   // Make `cnt` items of level l (already in this warp's level-l storage,
-  // prefix already in W.phi) this warp's new base subtree.
+  // prefix already in W.phi, plan in W.plan) this warp's new base subtree.
   __device__ void install(int l, int cnt) {
     if (lane == 0) {
       for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
@@ -455,14 +547,13 @@ struct Engine {
   }
 
   // Steal half of the remaining items at the shallowest level of another
-  // warp of this CTA.  The thief copies the victim's prefix and the upper
-  // half of its items, then CASes the victim's word (gen | next | end) down
-  // to the split point; the copy is valid iff the CAS succeeds, because the
-  // victim rewrites its items or prefix only after bumping gen.  Returns the
-  // level (1 = edge pairs) or 0.
+  // warp of this CTA.  The thief copies the victim's plan, prefix and the
+  // upper half of its items, takes a hold on the victim's slot, then CASes
+  // the victim's word (gen | next | end) down to the split point.  The copy is
+  // valid iff the CAS succeeds: a warp rewrites its items, prefix, plan or
+  // slot only after bumping gen.  Returns the level (1 = edge pairs) or 0.
   __device__ int steal_local(int nwarps, int me) {
-    const int k = P.k;
-    for (int l = 1; l <= k - 2; ++l) {
+    for (int l = 1; l <= kMaxK - 2; ++l) {
       int rem = 0, vic = -1;
       if (lane < nwarps && lane != me) {
         const unsigned long long w = *(volatile unsigned long long *)&warp_at(lane).word[l];
@@ -484,8 +575,15 @@ struct Engine {
       __threadfence_block();
       const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
       if (n - it < 2) continue;
+      const int vslot = *(volatile int32_t *)&V.slot;
+      if (vslot < 0) continue;
       const int take = (n - it) / 2;
       const int from = n - take;
+      {  // plan
+        const volatile int32_t *sp = reinterpret_cast<const volatile int32_t *>(&V.plan);
+        int32_t *dp = reinterpret_cast<int32_t *>(&W.plan);
+        for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dp[t] = sp[t];
+      }
       if (l == 1) {
         if (lane < take) {
           W.er[lane] = ((volatile int32_t *)V.er)[from + lane];
@@ -500,8 +598,18 @@ struct Engine {
       __threadfence_block();
       __syncwarp();
       int won = 0;
-      if (lane == 0) won = atomicCAS(&V.word[l], w, (w & ~0xffffull) | (unsigned long long)from) == w;
+      if (lane == 0) {
+        atomicAdd(&tab->hot[vslot].holders, 1);
+        won = atomicCAS(&V.word[l], w, (w & ~0xffffull) | (unsigned long long)from) == w;
+        if (won) {
+          W.slot = vslot;
+        } else {
+          release_lane0(vslot);  // nothing to flush: this warp holds no work
+          W.slot = -1;           // the plan copy above overwrote the old one
+        }
+      }
       won = __shfl_sync(kFull, won, 0);
+      __syncwarp();
       if (won) {
         install(l, take);
         if (lane == 0) atomicAdd(&ctl->steals, 1ull);
@@ -532,12 +640,14 @@ struct Engine {
     return -1;
   }
 
-  // Write a unit: level l, prefix W.phi[0..l-1], items [from, from+cnt) of
-  // level l (pairs when l == 1).
+  // Write a unit: slot, level l, prefix W.phi[0..l-1], items [from, from+cnt)
+  // of level l (pairs when l == 1).  A unit with items carries one hold on
+  // its slot.
   __device__ void queue_publish(unsigned long long pos, int l, int from, int cnt) {
     SplitUnit &u = units[pos & (kQueueCap - 1)];
     u.level = l;
     u.nitems = cnt;
+    u.slot = W.slot;
     if (l == 1) {
       for (int t = 0; t < cnt; ++t) {
         u.items[2 * t] = W.er[from + t];
@@ -552,9 +662,10 @@ struct Engine {
     atomicExch(&qh->seq[pos & (kQueueCap - 1)], pos + 1);
   }
 
-  // Pop one unit into this warp's state; returns its level or 0.
+  // Pop one unit into this warp's state; returns its level or 0.  The
+  // unit's hold on its slot passes to this warp.
   __device__ int queue_pop() {
-    int l = 0, cnt = 0;
+    int l = 0, cnt = 0, us = -1;
     if (lane == 0) {
       unsigned long long pos = *(volatile unsigned long long *)&qh->head;
       for (int tries = 0; tries < 64; ++tries) {
@@ -568,17 +679,18 @@ struct Engine {
             const volatile SplitUnit &u = units[slot];
             l = u.level;
             cnt = u.nitems;
-            if (l == 1 && cnt > 0 && 2 * cnt <= kUnitItems) {
+            us = u.slot;
+            if (us < 0 || cnt <= 0 || l < 1 || l > kMaxK - 2 || (l == 1 ? 2 * cnt : cnt) > kUnitItems) {
+              l = 0;  // an empty reservation (it carries no hold)
+            } else if (l == 1) {
               for (int t = 0; t < cnt; ++t) {
                 W.er[t] = u.items[2 * t];
                 W.ec[t] = u.items[2 * t + 1];
               }
-            } else if (l >= 2 && l <= P.k - 2 && cnt > 0 && cnt <= kUnitItems) {
-              for (int j = 0; j < l; ++j) W.phi[j] = u.phi[j];
-              int32_t *mb = buf(l);
-              for (int t = 0; t < cnt; ++t) mb[t] = u.items[t];
             } else {
-              l = 0;
+              for (int j = 0; j < l; ++j) W.phi[j] = u.phi[j];
+              int32_t *mb = buf(l);  // buffer placement does not depend on the plan
+              for (int t = 0; t < cnt; ++t) mb[t] = u.items[t];
             }
             __threadfence();
             atomicExch(&qh->seq[slot], pos + kQueueCap);
@@ -594,8 +706,10 @@ struct Engine {
     }
     l = __shfl_sync(kFull, l, 0);
     cnt = __shfl_sync(kFull, cnt, 0);
+    us = __shfl_sync(kFull, us, 0);
     __syncwarp();
     if (!l) return 0;
+    load_plan(us);
     install(l, cnt);
     return l;
   }
@@ -632,6 +746,7 @@ struct Engine {
             }
             w = old;
           }
+          if (cnt) atomicAdd(&tab->hot[W.slot].holders, 1);  // the unit's hold
           queue_publish((unsigned long long)pos, l, from, cnt);
           if (cnt) atomicAdd(&ctl->splits, 1ull);
         }
@@ -640,87 +755,68 @@ struct Engine {
     __syncwarp();
   }
 
-  __device__ __forceinline__ unsigned long long now_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-  }
-
   // ---- main loop ------------------------------------------------------------
   // level 1 iterates edge pairs, 2..k-2 iterate buffered candidates, the last
   // vertex k-1 is counted in place.  `base` is the shallowest level this warp
-  // owns: below it the warp acquires new work (an edge chunk, a steal from
-  // its CTA, or a unit from the global ring).
+  // owns: below it the warp releases its slot and acquires new work (level-0
+  // tickets of an open slot, a steal from its CTA, or a unit from the ring).
   __device__ void run(int nwarps, int me) {
-    const int k = P.k;
     int level = 0, base = 1;
-    bool edges_left = true;
-    bool busy = true;     // counted in ctl->pending (warps that hold work)
     bool hungry = false;  // counted in ctl->hungry (warps polling for work)
+    bool holding = false;
     unsigned claims = 0;
     if (lane == 0) {
       for (int l = 0; l < kStoredMax; ++l) W.word[l] = 0;
       for (int l = 0; l < kMaxK; ++l) W.h[l].complete = 0;
-      if (cfg.steal) atomicAdd(&ctl->pending, 1);
+      W.slot = -1;
     }
     __syncwarp();
     for (;;) {
       if (level < base) {
-        // ---- acquire new work ----
-        level = 0;
-        if (edges_left) {
-          if (fetch_edges()) level = base = 1;
-          else edges_left = false;
+        // ---- release the finished subtree, then acquire new work ----
+        if (holding) {
+          if (lane == 0) release_lane0(W.slot);
+          __syncwarp();
+          holding = false;
         }
+        level = 0;
+        if (take_tickets()) level = base = 1;
         if (!level && cfg.steal) {
-          const unsigned long long t0 = now_ns();
-          unsigned nap = 256;
-          for (;;) {
-            int l = steal_local(nwarps, me);
-            // one look at the ring: pop only when it holds units; retire when
-            // it is empty and no warp holds work
-            int state = 0;  // 0 wait, 1 ring non-empty, 2 done
-            if (!l && lane == 0) {
+          int l = steal_local(nwarps, me);
+          if (!l) {
+            int nonempty = 0;
+            if (lane == 0) {
               const unsigned long long h = *(volatile unsigned long long *)&qh->head;
               const unsigned long long t = *(volatile unsigned long long *)&qh->tail;
-              if (h < t) state = 1;
-              else if (*(volatile int32_t *)&ctl->pending <= (busy ? 1 : 0)) state = 2;
+              nonempty = h < t;
             }
-            state = __shfl_sync(kFull, state, 0);
-            if (!l && state == 1) l = queue_pop();
-            if (l) {
-              level = base = l;
-              break;
-            }
-            if (lane == 0) {
-              if (busy) atomicSub(&ctl->pending, 1);
-              if (!hungry) atomicAdd(&ctl->hungry, 1);
-            }
-            busy = false;
-            hungry = true;
-            int done = state == 2;
-            // bounded wait: a warp idle for longer than the limit reports a
-            // timeout instead of spinning on (no work is lost: the busy warps
-            // drain the ring before they retire)
-            if (!done && lane == 0 && now_ns() - t0 > (unsigned long long)cfg.idle_ms * 1000000ull) {
-              raise_error(ctl, TDFS_ERR_TIMEOUT);
-              done = 1;
-            }
-            done = __shfl_sync(kFull, done, 0);
-            if (done) break;
-            __nanosleep(nap);
-            nap = min(nap * 2, 8192u);
+            if (__shfl_sync(kFull, nonempty, 0)) l = queue_pop();
           }
-          if (level && lane == 0) {
-            if (!busy) atomicAdd(&ctl->pending, 1);
-            if (hungry) atomicSub(&ctl->hungry, 1);
-          }
-          if (level) {
-            busy = true;
-            hungry = false;
-          }
+          if (l) level = base = l;
         }
-        if (!level) break;
+        if (level) {
+          holding = true;
+          if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
+          hungry = false;
+          idle_since = 0;
+          nap = 256;
+          continue;
+        }
+        // ---- idle: retire when every admitted slot is done and no more will
+        // come; otherwise wait (bounded) for splits or admissions
+        int done = 0;
+        if (lane == 0) {
+          if (!hungry && cfg.steal) atomicAdd(&ctl->hungry, 1);
+          const SlotCtl &C = tab->ctl;
+          const unsigned long long adm = *(volatile unsigned long long *)&C.admitted;
+          const unsigned long long cmp = *(volatile unsigned long long *)&C.completed;
+          const int shut = *(volatile int32_t *)&C.shutdown;
+          if (shut && cmp >= adm) done = 1;
+        }
+        hungry = cfg.steal != 0;
+        done = __shfl_sync(kFull, done, 0);
+        if (done) break;
+        if (!wait_for_work()) break;
         continue;
       }
       const int32_t idx = claim(level);
@@ -739,8 +835,8 @@ struct Engine {
         }
         __syncwarp();
         if (cfg.steal && ((++claims & 7u) == 0)) maybe_donate(level);
-        if (level + 1 == k - 1) {
-          count += count_last(k - 1);
+        if (level + 1 == P.k - 1) {
+          count += count_last(P.k - 1);
         } else {
           setup(level + 1, true);
           produce(level + 1);
@@ -754,19 +850,42 @@ struct Engine {
       }
       --level;
     }
-    if (lane == 0 && cfg.steal) {
-      if (busy) atomicSub(&ctl->pending, 1);
-      if (hungry) atomicSub(&ctl->hungry, 1);
-    }
+    if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
     __syncwarp();
+  }
+
+  // Bounded idle wait between acquisition attempts: exponential back-off.
+  // Returns false (retire) after too long without work: in a launch whose
+  // admissions are closed that means a busy warp stalled and is reported as
+  // a timeout; a serving launch simply retires and the host relaunches it.
+  unsigned nap = 256;
+  unsigned long long idle_since = 0;
+  __device__ bool wait_for_work() {
+    int ok = 1;
+    if (lane == 0) {
+      const unsigned long long t = now_ns();
+      if (!idle_since) idle_since = t;
+      const SlotCtl &C = tab->ctl;
+      const int shut = *(volatile int32_t *)&C.shutdown;
+      const unsigned long long limit_ms = shut ? (unsigned long long)cfg.idle_ms : (unsigned long long)C.idle_exit_ms;
+      if (t - idle_since > limit_ms * 1000000ull) {
+        if (shut) raise_error(ctl, TDFS_ERR_TIMEOUT);
+        ok = 0;
+      }
+    }
+    ok = __shfl_sync(kFull, ok, 0);
+    if (ok) {
+      __nanosleep(nap);
+      nap = min(nap * 2, 8192u);
+    }
+    return ok;
   }
 };
 
 template <bool LAB>
-__global__ void __launch_bounds__(256) match_kernel(const __grid_constant__ DevPlan P,
-                                                    const __grid_constant__ DevGraph G,
+__global__ void __launch_bounds__(256) match_kernel(const __grid_constant__ DevGraph G,
                                                     const __grid_constant__ KernelCfg cfg, RunCtl *ctl,
-                                                    SplitUnit *units, QueueHdr *qh) {
+                                                    SlotTable *tab, SplitUnit *units, QueueHdr *qh) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int me = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
@@ -775,27 +894,21 @@ __global__ void __launch_bounds__(256) match_kernel(const __grid_constant__ DevP
   const size_t hdr = (sizeof(WarpSmem) + 15) & ~(size_t)15;
   int32_t *win = reinterpret_cast<int32_t *>(base + hdr);
   int32_t *bufs = win + cfg.window;
-  Engine<LAB> eng(P, G, cfg, ctl, units, qh, W, bufs, win);
+  Engine<LAB> eng(G, cfg, ctl, tab, units, qh, W, bufs, win);
   eng.run(nwarps, me);
-  unsigned long long c = eng.count;
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&ctl->count, c);
 }
 
-__global__ void init_kernel(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin) {
+__global__ void init_kernel(RunCtl *ctl, QueueHdr *qh) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t == 0) {
-    ctl->edge_next = 0;
-    ctl->count = 0;
+    ctl->hungry = 0;
     ctl->steals = 0;
     ctl->splits = 0;
     ctl->error = 0;
-    ctl->pending = 0;  // warps add themselves when they start
-    ctl->hungry = 0;
     qh->head = 0;
     qh->tail = 0;
   }
   for (int i = t; i < kQueueCap; i += gridDim.x * blockDim.x) qh->seq[i] = (unsigned long long)i;
-  (void)e_begin;
 }
 
 }  // namespace
@@ -821,24 +934,18 @@ int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem) {
   return e == cudaSuccess ? n : -1;
 }
 
-void init_launch(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin, cudaStream_t stream) {
-  init_kernel<<<64, 256, 0, stream>>>(ctl, qh, total_warps, e_begin);
+void init_launch(RunCtl *ctl, QueueHdr *qh, cudaStream_t stream) {
+  init_kernel<<<64, 256, 0, stream>>>(ctl, qh);
 }
 
-int launch_match(const DevPlan &plan, const DevGraph &g, RunCtl *ctl, SplitUnit *units, QueueHdr *qh,
+int launch_match(bool labeled, const DevGraph &g, RunCtl *ctl, SlotTable *tab, SplitUnit *units, QueueHdr *qh,
                  const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream) {
   const size_t smem = (size_t)cfg.warp_bytes * warps_per_block;
-  cudaError_t e;
-  if (plan.labeled) {
-    e = cudaFuncSetAttribute(match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      match_kernel<true><<<blocks, warps_per_block * 32, smem, stream>>>(plan, g, cfg, ctl, units, qh);
-  } else {
-    e = cudaFuncSetAttribute(match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      match_kernel<false><<<blocks, warps_per_block * 32, smem, stream>>>(plan, g, cfg, ctl, units, qh);
-  }
-  if (e == cudaSuccess) e = cudaGetLastError();
+  if (labeled)
+    match_kernel<true><<<blocks, warps_per_block * 32, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+  else
+    match_kernel<false><<<blocks, warps_per_block * 32, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+  const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "match kernel launch: %s", cudaGetErrorString(e));
   return TDFS_OK;
 }

@@ -57,14 +57,16 @@ constexpr int kEdgeChunk = 32;  // directed edges per level-0 ticket
 
 size_t warp_smem_bytes(int k, int cap, int window);
 
-// Launch the counting kernel for one plan.  `ctl` must have been initialised
-// by init_launch on the same stream.
-int launch_match(const DevPlan &plan, const DevGraph &g, RunCtl *ctl, SplitUnit *units, QueueHdr *qh,
-                 const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream);
 // CTAs of the match kernel that fit on one SM at once (registers, shared
 // memory, threads); -1 on a CUDA error.  The persistent grid must not exceed
 // this times the SM count: idle warps wait for busy ones.
 int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem);
-void init_launch(RunCtl *ctl, QueueHdr *qh, int total_warps, int64_t e_begin, cudaStream_t stream);
+
+// Reset the control block and the split ring (stream-ordered).
+void init_launch(RunCtl *ctl, QueueHdr *qh, cudaStream_t stream);
+
+// Launch the match kernel over the slot table `tab` (filled by the host).
+int launch_match(bool labeled, const DevGraph &g, RunCtl *ctl, SlotTable *tab, SplitUnit *units, QueueHdr *qh,
+                 const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream);
 
 }  // namespace tdfs

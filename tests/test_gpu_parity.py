@@ -172,3 +172,25 @@ def test_reference_build_counts(T):
             assert got == T.count(dev[r["graph"]], P, T.default_options(steal=0, merge_window=-1)).count
             continue
         assert got == bad.get(key, r["count"]), r
+
+
+def test_batch_equals_single_launches(er, cl, T):
+    """Many plans of uneven size in one launch (one slot per plan, labeled
+    and unlabeled mixed in one call) give the same counts as one launch each."""
+    rng = random.Random(11)
+    for case in (er, cl):
+        texts = [(TRIANGLE, False), (CYCLE4, False), (clique(4), False), (HOUSE, False), (clique(5), False)]
+        texts += [(random_pattern(3 + t % 5, 0.5, 4, rng), t % 2 == 0) for t in range(12)]
+        plans = [T.PatternPreprocessor(text=t, labeled=lab) for t, lab in texts]
+        batch, _ = T.count_batch(case.dev, plans)
+        assert batch == [T.count(case.dev, p).count for p in plans]
+
+
+def test_batch_on_edge_ranges(cl, T):
+    """Batched slots honour the option's edge range like single launches."""
+    plans = [T.PatternPreprocessor(text=t) for t in (TRIANGLE, CYCLE4, clique(4))]
+    e = cl.csr.nedges
+    parts = [T.count_batch(cl.dev, plans, T.default_options(edge_begin=b, edge_end=min(e, b + e // 3 + 1)))[0]
+             for b in range(0, e, e // 3 + 1)]
+    whole, _ = T.count_batch(cl.dev, plans)
+    assert [sum(p[i] for p in parts) for i in range(3)] == whole
