@@ -3,10 +3,13 @@
 
     python bench.py [--gpus N --steps K --warmup W] [--workload c2] [--impl tdfs|reference]
 
-One step = one full count of every pattern of the workload over the whole
-data graph (all level-0 edges), the graph already resident in HBM.  With N
-ranks (torchrun, one process per GPU) the level-0 edge chunks are dealt
-round-robin over the ranks (strong scaling, one u64 all-reduce per step).
+One step = every pattern of the workload counted over one batch of level-0
+edges, the graph already resident in HBM: the whole edge array for the small
+configs, one contiguous 1/1000 slice of it for the power-law config (its
+house count is ~1e13 matches, about 25 GPU-minutes for the whole graph), the
+timed slices spread evenly over the array.  With N ranks (torchrun, one
+process per GPU) the level-0 edge chunks of each step are dealt round-robin
+over the ranks (strong scaling, one u64 all-reduce per step).
 
 The JSON line reports
   value       matches/s of the device-timed steps (CUDA events, max over ranks)
@@ -14,12 +17,12 @@ The JSON line reports
               graph upload from pinned host memory + counts + read-back
   roofline    merge-model algorithmic bytes per match-kernel launch / mean
               launch time, against the measured HBM copy bandwidth
-  cpu_baseline the multithreaded CPU oracle on a bounded edge shard
+  cpu_baseline the multithreaded CPU oracle on a bounded prefix of a step
   clocks      nvidia-smi SM clocks and throttle reasons sampled while timing
 
---impl reference runs the reference's own CUDA build (oracle/_ref/ulb.out,
-lb.out, compiled from the reference sources for sm_100a) on the same graph
-written in its file format, reading its own kernel timing line.
+--impl reference runs the reference's own CUDA kernel (built from the
+reference sources for sm_100a into oracle/_ref/) on the same graph, written in
+its file format, over the same edge ranges, reading its own kernel timing.
 """
 from __future__ import annotations
 
@@ -51,22 +54,40 @@ def clique(k):
 
 
 def workload(name, T):
-    """(description dict, host CSR, [(pattern name, text)], labeled)."""
+    """(description, host CSR, [(pattern name, text)], labeled, slices).
+
+    slices = S: one step counts every pattern over one contiguous 1/S slice of
+    the level-0 directed-edge array (S = 1: the whole graph)."""
     if name == "c1":
         g = T.gen_er(4096, 16.0, 0)
         pats = [("triangle", TRIANGLE), ("4-cycle", CYCLE4), ("diamond", DIAMOND), ("4-clique", clique(4))]
-        return ({"workload": "ER n=4096 avg-degree 16 seed 0; triangle, 4-cycle, diamond, 4-clique"}, g, pats, False)
+        return ({"workload": "ER n=4096 avg-degree 16 seed 0; triangle, 4-cycle, diamond, 4-clique; "
+                             "one step = every pattern over the whole graph"}, g, pats, False, 1)
     if name == "c2":
         g = T.gen_chung_lu(1_100_000, 3_000_000, 2.1, 30_000, 1)
         pats = [("5-clique", clique(5)), ("house", HOUSE)]
-        return ({"workload": "Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1, degree-ordered ids; 5-clique, house"},
-                g, pats, False)
+        return ({"workload": "Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1, degree-ordered ids; 5-clique and "
+                             "house; one step = both patterns over one contiguous 1/1000 slice of the level-0 "
+                             "edge array, timed slices spread evenly over the array"}, g, pats, False, 1000)
     if name == "c3":
         g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
         pats = [(f"labeled-{i}", T.gen_pattern(6 + i % 2, 0.4, 4, 3 * 1000 + i)) for i in range(8)]
         return ({"workload": "ER n=4096 avg-degree 16 seed 0, labels U[0,4) seed 2; 8 random 6-7 vertex labeled "
-                             "patterns (density 0.4, seed 3)"}, g, pats, True)
+                             "patterns (density 0.4, seed 3); one step = every pattern over the whole graph"},
+                g, pats, True, 1)
     raise SystemExit(f"unknown workload {name}")
+
+
+def step_ranges(nedges, slices, steps, warmup):
+    """Edge ranges of the warm-up and timed steps."""
+    if slices == 1:
+        return [(0, nedges)] * warmup, [(0, nedges)] * steps
+
+    def rng(j):
+        return (j * nedges // slices, (j + 1) * nedges // slices)
+    timed = [rng(int((s + 0.5) * slices / steps)) for s in range(steps)]
+    warm = [rng(int((w + 0.5) * slices / max(1, warmup)) + 1) for w in range(warmup)]
+    return warm, timed
 
 
 class ClockSampler:
@@ -122,25 +143,37 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(g, pats, labeled, shard):
-    """The CPU oracle (multithreaded DFS, same plan) on 1/shard of the level-0
-    edge chunks.  Returns (record, model bytes, matches) of the sample."""
+def cpu_baseline(g, pats, labeled, rng, budget_s=12.0):
+    """The CPU oracle (multithreaded DFS, same plan and semantics) on a
+    bounded sample of the first timed step: for each pattern, growing prefixes
+    of that step's edge range until about budget_s / len(pats) seconds are
+    spent.  Returns (record, {pattern: (model bytes, matches)})."""
     from oracle import pyoracle as po
-    import tdfs_b200 as T
     G = po.Graph(g.rowptr, g.colidx, g.labels if labeled else None)
     threads = os.cpu_count() or 1
-    total = byts = 0
-    t0 = time.perf_counter()
-    for _, text in pats:
+    b0, e0 = rng
+    per = {}
+    total = 0
+    spent = 0.0
+    done_edges = []
+    for name, text in pats:
         P = po.Plan(text, labeled)
-        for b, e in T.shard_edge_ranges(g.nedges, 0, shard):
-            c, nb = po.count(G, P, threads, b, e, with_bytes=True)
-            total += c
+        lo, span, byts, cnt, t_pat = b0, 32, 0, 0, 0.0
+        while lo < e0 and t_pat < budget_s / len(pats):
+            hi = min(e0, lo + span)
+            t0 = time.perf_counter()
+            c, nb = po.count(G, P, threads, lo, hi, with_bytes=True)
+            t_pat += time.perf_counter() - t0
+            cnt += c
             byts += nb
-    dt = time.perf_counter() - t0
-    return ({"value": total / dt if dt > 0 else None, "unit": "matches/s", "cores": threads, "kind": "port",
-             "sample": f"level-0 edge chunks t % {shard} == 0 (1/{shard} of the edges), every pattern",
-             "seconds": round(dt, 2)}, byts, total)
+            lo, span = hi, span * 2
+        per[name] = (byts, cnt)
+        total += cnt
+        spent += t_pat
+        done_edges.append(f"{name}: edges [{b0}, {lo})")
+    return ({"value": total / spent if spent > 0 else None, "unit": "matches/s", "cores": threads, "kind": "port",
+             "sample": "CPU oracle, all host threads, on prefixes of the first timed step's edge range (" +
+                       "; ".join(done_edges) + ")", "seconds": round(spent, 2)}, per)
 
 
 def run_tdfs(args, rank, world, dist):
@@ -148,51 +181,51 @@ def run_tdfs(args, rank, world, dist):
     import tdfs_b200 as T
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    desc, g, pats, labeled = workload(args.workload, T)
+    desc, g, pats, labeled, slices = workload(args.workload, T)
     G = T.GraphPreprocessor(csr=g, labeled=labeled, device=dev)
     plans = [(n, T.PatternPreprocessor(text=t, labeled=labeled)) for n, t in pats]
-    opt = T.shard_options(rank, world)
+    warm_r, timed_r = step_ranges(g.nedges, slices, args.steps, args.warmup)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
-    def step():
-        out = []
-        for n, p in plans:
-            r = T.count(G, p, opt)
-            out.append(r)
-        return out
+    def opts(rng):
+        return T.shard_options(rank, world, edge_begin=rng[0], edge_end=rng[1])
 
-    for _ in range(args.warmup):
-        step()
+    def step(graph, rng):
+        return [T.count(graph, p, opts(rng)) for _, p in plans]
+
+    for r in warm_r:
+        step(G, r)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    step_ms, launch_ms, matches = [], [], 0
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in timed_r]
+    launch = []        # (pattern, kernel ms, count) per match-kernel launch
+    per_pattern = {n: 0 for n, _ in plans}
     torch.cuda.synchronize()
-    for s in range(args.steps):
+    for s, r in enumerate(timed_r):
         flush.zero_()  # L2 flush between timed steps (256 MB > 126 MB L2), outside the events
         ev[s][0].record()
-        res = step()
+        res = step(G, r)
         ev[s][1].record()
-        launch_ms += [r.kernel_ms for r in res]
-        matches += sum(r.count for r in res)
+        for (n, _), x in zip(plans, res):
+            launch.append((n, x.kernel_ms, x.count))
+            per_pattern[n] += x.count
     torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     if dist:
         dist.barrier()
     clk = clocks.stop()
     total_ms = sum(step_ms)
-    per_pattern = {n: r.count for (n, _), r in zip(plans, res)}
     if dist:
         t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-        m = torch.tensor([matches] + list(per_pattern.values()), dtype=torch.int64, device="cuda")
+        m = torch.tensor(list(per_pattern.values()), dtype=torch.int64, device="cuda")
         dist.all_reduce(m)
-        matches = int(m[0].item())
-        per_pattern = {n: int(v) for n, v in zip(per_pattern, m[1:].tolist())}
+        per_pattern = {n: int(v) for n, v in zip(per_pattern, m.tolist())}
+    matches = sum(per_pattern.values())
     value = matches / (total_ms / 1e3)
 
     # ---- end to end through the C ABI with host buffers ------------------
@@ -200,22 +233,21 @@ def run_tdfs(args, rank, world, dist):
     ci = torch.from_numpy(np.ascontiguousarray(g.colidx)).pin_memory()
     lb = torch.from_numpy(np.ascontiguousarray(g.labels)).pin_memory() if labeled else None
     h2d = rp.numel() * 8 + ci.numel() * 4 + (lb.numel() * 4 if lb is not None else 0) + sum(len(t) for _, t in pats)
-    d2h = 64 * len(pats)  # the launch control block read back per count
-    e2e_s, e2e_m = [], 0
-    for s in range(max(1, args.steps)):
+    d2h = 8 * len(pats)  # one u64 count read back per pattern
+    e2e_s, e2e_m = 0.0, 0
+    for r in timed_r:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         Gh = T.GraphPreprocessor(rowptr=rp.numpy(), colidx=ci.numpy(), labels=None if lb is None else lb.numpy(),
                                  labeled=labeled, device=dev)
         ps = [T.PatternPreprocessor(text=t, labeled=labeled) for _, t in pats]
-        e2e_m += sum(T.count(Gh, p, opt).count for p in ps)
+        e2e_m += sum(T.count(Gh, p, opts(r)).count for p in ps)
         Gh.close()
-        e2e_s.append(time.perf_counter() - t0)
-    e2e_total = sum(e2e_s)
+        e2e_s += time.perf_counter() - t0
     if dist:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
+        e2e_s = float(t.item())
         m = torch.tensor([e2e_m], dtype=torch.int64, device="cuda")
         dist.all_reduce(m)
         e2e_m = int(m.item())
@@ -225,75 +257,80 @@ def run_tdfs(args, rank, world, dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32/u64",
         "data": "synthetic (seeded generators of the benchmark config)",
-        "config": dict(desc, parallelism=f"level-0 edge chunks round-robin over {world} rank(s)",
-                       l2="flushed between timed steps (256 MB write)", counts=per_pattern),
-        "e2e": {"value": e2e_m / e2e_total, "unit": "matches/s", "h2d_bytes_per_step": h2d,
+        "config": dict(desc, parallelism=f"level-0 edge chunks dealt round-robin over {world} rank(s)",
+                       l2="flushed between timed steps (256 MB write)", timed_edge_ranges=timed_r,
+                       counts=per_pattern),
+        "e2e": {"value": e2e_m / e2e_s, "unit": "matches/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 2 * len(pats) * args.steps,
         "clocks": clk,
     }
-    return line, launch_ms, (g, pats, labeled)
+    return line, launch, (g, pats, labeled, timed_r)
 
 
 def run_reference(args, rank, world):
-    """The reference's own CUDA build on the same workload."""
+    """The reference's own CUDA kernel on the same steps: oracle/_ref/refshard_*
+    drives _parallel_match (src/gpu_match.cu, compiled unchanged for sm_100a)
+    over the same edge ranges and reports its own cudaEvent kernel time."""
     import tdfs_b200 as T
     if rank != 0:
         return None
-    exe = os.path.join(ROOT, "oracle", "_ref", "lb.out" if args.workload == "c3" else "ulb.out")
+    desc, g, pats, labeled, slices = workload(args.workload, T)
+    exe = os.path.join(ROOT, "oracle", "_ref", "refshard_lb" if labeled else "refshard_ulb")
     if not os.path.exists(exe):
         return {"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources)"}
-    desc, g, pats, labeled = workload(args.workload, T)
+    warm_r, timed_r = step_ranges(g.nedges, slices, args.steps, args.warmup)
     work = tempfile.mkdtemp(prefix="tdfs_ref_")
     prefix = os.path.join(work, "snap.txt")
     g.write(prefix)
-    files = []
-    for n, t in pats:
-        p = os.path.join(work, n + ".g")
-        with open(p, "w") as f:
-            f.write(t)
-        files.append((n, p))
 
-    def step():
-        ms, cnt, out = 0.0, 0, {}
-        for n, p in files:
-            r = subprocess.run([exe, prefix, p], capture_output=True, text=True, timeout=args.ref_timeout)
-            last = [l for l in r.stdout.splitlines() if l.count("\t") == 2][-1]
-            _, m, c = last.split("\t")
-            ms += float(m)
-            cnt += int(c)
-            out[n] = int(c)
-        return ms, cnt, out
+    def run(text, ranges):
+        p = os.path.join(work, "p.g")
+        with open(p, "w") as f:
+            f.write(text)
+        args_r = [str(x) for r in ranges for x in r]
+        r = subprocess.run([exe, prefix, p] + args_r, capture_output=True, text=True, timeout=args.ref_timeout)
+        lines = [l for l in r.stdout.splitlines() if l.count("\t") == 2]
+        if r.returncode or not lines:
+            raise RuntimeError(f"reference run failed rc={r.returncode}: {r.stderr[-300:]}")
+        _, ms, c = lines[-1].split("\t")
+        return float(ms), int(c)
 
     try:
-        for _ in range(args.warmup):
-            step()
-        tot_ms, tot_c = 0.0, 0
-        for _ in range(args.steps):
-            ms, c, counts = step()
+        for _, t in pats:
+            run(t, warm_r)
+        tot_ms, tot_c, counts = 0.0, 0, {}
+        for n, t in pats:
+            ms, c = run(t, timed_r)
             tot_ms += ms
             tot_c += c
+            counts[n] = c
     except subprocess.TimeoutExpired:
-        return {"impl": "reference", "unavailable": f"reference build exceeded {args.ref_timeout}s per pattern"}
+        return {"impl": "reference", "unavailable": f"reference kernel exceeded {args.ref_timeout}s on the workload"}
+    except RuntimeError as e:
+        return {"impl": "reference", "unavailable": str(e)[:200]}
     value = tot_c / (tot_ms / 1e3)
     return {"impl": "reference", "metric": "matches_per_s", "value": value, "unit": "matches/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32/u64",
-            "data": "synthetic", "config": dict(desc, counts=counts, timing="the reference's own cudaEvent pair "
-                                                 "around its kernel (cu_test.cu:81-97)"),
+            "data": "synthetic (seeded generators of the benchmark config)",
+            "config": dict(desc, counts=counts, timed_edge_ranges=timed_r,
+                           timing="the reference's own kernel, cudaEvent pair around each launch as cu_test.cu:81-97",
+                           note="the reference build's counts can differ from the reference semantics on heavy "
+                                "subtrees; they are reported as printed"),
             "cpu_baseline": {"value": value, "unit": "matches/s", "cores": 0, "kind": "reference",
-                             "sample": "the reference's CUDA build on the GPU (it has no CPU path)"},
+                             "sample": "the reference's own CUDA kernel on the timed steps (it has no CPU path)"},
             "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
     ap.add_argument("--impl", default="tdfs", choices=["tdfs", "reference"])
-    ap.add_argument("--cpu-shard", type=int, default=0, help="CPU baseline sample: 1/shard of the edge chunks")
+    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-oracle work for cpu_baseline")
     ap.add_argument("--ref-timeout", type=int, default=600)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
@@ -302,32 +339,41 @@ def main():
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl" if args.impl == "tdfs" else "gloo", timeout=datetime.timedelta(seconds=600))
+        if args.impl == "tdfs":
+            import torch
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl" if args.impl == "tdfs" else "gloo", timeout=datetime.timedelta(seconds=900))
     if args.impl == "reference":
         line = run_reference(args, rank, world)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if dist:
+            dist.barrier()
             dist.destroy_process_group()
         return
-    line, launch_ms, (g, pats, labeled) = run_tdfs(args, rank, world, dist)
+    line, launch, (g, pats, labeled, timed_r) = run_tdfs(args, rank, world, dist)
     if rank == 0:
         peak, kind = measured_hbm_peak()
-        shard = args.cpu_shard or {"c1": 1, "c3": 1, "c2": 2000}.get(args.workload, 1000)
+        per = {}
         if world == 1:
-            cb, model_bytes, sample_matches = cpu_baseline(g, pats, labeled, shard)
+            cb, per = cpu_baseline(g, pats, labeled, timed_r[0], args.cpu_budget)
             line["cpu_baseline"] = cb
         else:
             line["cpu_baseline"] = None
-            model_bytes = sample_matches = 0
-        mean_launch_s = statistics.mean(launch_ms) / 1e3 if launch_ms else None
-        if sample_matches and mean_launch_s:
-            per_match = model_bytes / sample_matches
-            per_launch = per_match * line["value"] * (sum(launch_ms) / 1e3) / len(launch_ms)
-            achieved = per_launch / mean_launch_s / 1e9
+        # roofline of the match kernel: merge-model bytes per match (oracle
+        # sample, per pattern) x matches per launch / mean launch time
+        usable = [(n, ms, c) for n, ms, c in launch if n in per and per[n][1] > 0 and ms > 0]
+        if usable:
+            bytes_launch = [per[n][0] / per[n][1] * c for n, ms, c in usable]
+            mean_b = statistics.mean(bytes_launch)
+            mean_s = statistics.mean(ms for _, ms, _ in usable) / 1e3
+            achieved = mean_b / mean_s / 1e9
             line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                 "frac": achieved / peak, "peak_kind": kind, "traffic": None,
-                                "bytes_model": "reference-plan merge model, bytes per match from the CPU sample"}
+                                "bytes_per_launch": mean_b, "mean_launch_ms": mean_s * 1e3,
+                                "bytes_model": "reference-plan merge model (4 B x (|set1|+|set2|) per set op, "
+                                               "16 B per list lookup, 8 B per level-0 edge); bytes per match "
+                                               "from the CPU-oracle sample, per pattern"}
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
