@@ -93,6 +93,40 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
 int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
                      const tdfs_options *opt, uint64_t *counts, float *kernel_ms);
 
+/* ---- serving (no reference counterpart; the north-star served stream) -----
+ * A continuous-batching server over one device-resident graph: queries
+ * submitted at any time are admitted into a running persistent kernel as
+ * in-flight places and device memory free up, so their work overlaps on the
+ * GPU.  Admission charges each query its slot record plus one CTA's DFS stack
+ * for its pattern size; a query that can never fit is rejected at submit with
+ * TDFS_ERR_ADMISSION.  While a server is attached, the graph handle must not
+ * be used for tdfs_count / tdfs_count_batch. */
+typedef struct tdfs_server tdfs_server;
+
+typedef struct {
+  int max_inflight;     /* queries on the device at once (<= 2048) */
+  int max_k;            /* largest pattern the stack layout holds (3..7) */
+  int labeled;          /* lb (1) or ulb (0) queries */
+  int idle_exit_ms;     /* the kernel retires after this long idle; relaunched on demand */
+  size_t mem_budget;    /* device bytes charged to in-flight queries (0 = max_inflight x a 7-vertex query) */
+  tdfs_options launch;  /* launch knobs; the edge range is ignored */
+} tdfs_server_options;
+
+typedef struct {
+  uint64_t completed;
+  uint64_t pending;     /* submitted, not yet admitted */
+  uint64_t inflight;    /* admitted, not yet complete */
+  double p50_us, p99_us, max_us;  /* submit -> completion seen on the host */
+  double queries_per_s; /* completed / (last completion - first submit) */
+} tdfs_serve_stats;
+
+void tdfs_server_options_default(tdfs_server_options *opt);
+int tdfs_server_create(tdfs_graph *g, const tdfs_server_options *opt, tdfs_server **out);
+int tdfs_server_submit(tdfs_server *s, const tdfs_plan *p, uint64_t *ticket); /* thread-safe */
+int tdfs_server_wait(tdfs_server *s, uint64_t ticket, uint64_t *count, double *latency_us);
+int tdfs_server_stats(tdfs_server *s, tdfs_serve_stats *st);
+int tdfs_server_destroy(tdfs_server *s); /* drains admitted queries, stops the kernel */
+
 /* ---- host CSR: generators and file writer (graph_converter/ output format,
  *      graph_converter/compactify.cpp:172-195, labelize.cpp:130-133) ------- */
 int tdfs_csr_read(const char *prefix, int labeled, tdfs_csr **out);

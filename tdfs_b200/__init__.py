@@ -36,6 +36,8 @@ EXPORTS = [
     "tdfs_count", "tdfs_count_batch",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
     "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern",
+    "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
+    "tdfs_server_stats", "tdfs_server_destroy",
 ]
 
 
@@ -58,6 +60,31 @@ class Options(C.Structure):
         ("edge_stride", C.c_int),
         ("edge_phase", C.c_int),
         ("stream", C.c_void_p),
+    ]
+
+
+class ServerOptions(C.Structure):
+    """tdfs_server_options."""
+    _fields_ = [
+        ("max_inflight", C.c_int),
+        ("max_k", C.c_int),
+        ("labeled", C.c_int),
+        ("idle_exit_ms", C.c_int),
+        ("mem_budget", C.c_size_t),
+        ("launch", Options),
+    ]
+
+
+class ServeStats(C.Structure):
+    """tdfs_serve_stats."""
+    _fields_ = [
+        ("completed", C.c_uint64),
+        ("pending", C.c_uint64),
+        ("inflight", C.c_uint64),
+        ("p50_us", C.c_double),
+        ("p99_us", C.c_double),
+        ("max_us", C.c_double),
+        ("queries_per_s", C.c_double),
     ]
 
 
@@ -99,6 +126,13 @@ def lib() -> C.CDLL:
     L.tdfs_gen_chung_lu.argtypes = [i64, i64, C.c_double, i32, C.c_uint64, pp]
     L.tdfs_gen_rmat.argtypes = [ci, ci, C.c_double, C.c_double, C.c_double, C.c_uint64, pp]
     L.tdfs_gen_pattern.argtypes = [ci, C.c_double, ci, C.c_uint64, C.c_char_p, C.c_size_t]
+    L.tdfs_server_options_default.argtypes = [C.POINTER(ServerOptions)]
+    L.tdfs_server_options_default.restype = None
+    L.tdfs_server_create.argtypes = [vp, C.POINTER(ServerOptions), pp]
+    L.tdfs_server_submit.argtypes = [vp, vp, C.POINTER(C.c_uint64)]
+    L.tdfs_server_wait.argtypes = [vp, C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(C.c_double)]
+    L.tdfs_server_stats.argtypes = [vp, C.POINTER(ServeStats)]
+    L.tdfs_server_destroy.argtypes = [vp]
     _lib = L
     return L
 
@@ -297,3 +331,47 @@ def shard_edge_ranges(nedges: int, rank: int, world: int):
             return out
         out.append((b, min(nedges, b + EDGE_CHUNK)))
         t += 1
+
+
+class Server:
+    """Continuous-batching query server over one device-resident graph
+    (tdfs_server_*): submit() admits queries into a running persistent
+    kernel; wait() returns (count, latency in microseconds)."""
+
+    def __init__(self, graph: GraphPreprocessor, labeled: bool = False, max_inflight: int = 256, max_k: int = 7,
+                 mem_budget: int = 0, idle_exit_ms: int = 50, **launch):
+        o = ServerOptions()
+        lib().tdfs_server_options_default(C.byref(o))
+        o.max_inflight, o.max_k, o.labeled = max_inflight, max_k, int(labeled)
+        o.mem_budget, o.idle_exit_ms = mem_budget, idle_exit_ms
+        for k, v in launch.items():
+            setattr(o.launch, k, v)
+        h = C.c_void_p()
+        _check(lib().tdfs_server_create(graph._h, C.byref(o), C.byref(h)))
+        self._h = h
+        self.graph = graph
+
+    def submit(self, pattern: PatternPreprocessor) -> int:
+        t = C.c_uint64()
+        _check(lib().tdfs_server_submit(self._h, pattern._h, C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int):
+        c, lat = C.c_uint64(), C.c_double()
+        _check(lib().tdfs_server_wait(self._h, ticket, C.byref(c), C.byref(lat)))
+        return c.value, lat.value
+
+    def stats(self) -> dict:
+        st = ServeStats()
+        _check(lib().tdfs_server_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServeStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            h, self._h = self._h, None
+            _check(lib().tdfs_server_destroy(h))
+
+    def __del__(self):
+        if _lib is not None and getattr(self, "_h", None):
+            _lib.tdfs_server_destroy(self._h)
+            self._h = None

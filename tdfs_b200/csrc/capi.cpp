@@ -15,6 +15,7 @@
 #include "graph.h"
 #include "match.cuh"
 #include "plan.h"
+#include "serve.h"
 
 struct tdfs_plan {
   tdfs::HostPlan host;
@@ -48,18 +49,14 @@ int fail(int code, const char *fmt, ...) {
 
 namespace {
 
-struct LaunchShape {
-  int warps_per_block;
-  int blocks;
-  KernelCfg cfg;
-};
-
 int cuda_err(cudaError_t e, const char *what) {
   return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
 // Choose the launch shape: a persistent grid of (resident CTAs per SM) x SMs.
-int plan_launch(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out) {
+}  // namespace
+
+int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out) {
   // device properties are queried once per device (the query costs ~ms)
   static cudaDeviceProp props[64];
   static bool have[64] = {};
@@ -99,6 +96,8 @@ int plan_launch(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options 
   return TDFS_OK;
 }
 
+namespace {
+
 // Level-0 tickets of an edge range dealt round-robin: ticket t covers the
 // chunk of 32 edges starting at e_begin + (t * stride + phase) * 32.
 int64_t ticket_count(int64_t b, int64_t e, int stride, int phase) {
@@ -123,7 +122,7 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   cudaError_t e = cudaSetDevice(g->device);
   if (e != cudaSuccess) return cuda_err(e, "cudaSetDevice");
   LaunchShape s;
-  int rc = plan_launch(g, kmax, labeled, o, &s);
+  int rc = launch_shape(g, kmax, labeled, o, &s);
   if (rc) return rc;
   const int64_t eb = std::max<int64_t>(0, o.edge_begin);
   const int64_t ee = (o.edge_end < 0 || o.edge_end > g->nedges) ? g->nedges : o.edge_end;
@@ -327,6 +326,50 @@ int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, c
   }
   if (kernel_ms) *kernel_ms = total;
   return TDFS_OK;
+}
+
+struct tdfs_server {
+  tdfs::Server *impl;
+};
+
+void tdfs_server_options_default(tdfs_server_options *o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof *o);
+  o->max_inflight = 256;
+  o->max_k = TDFS_MAX_PATTERN;
+  o->idle_exit_ms = 50;
+  tdfs_options_default(&o->launch);
+}
+
+int tdfs_server_create(tdfs_graph *g, const tdfs_server_options *opt, tdfs_server **out) {
+  if (!g || !out) return fail(TDFS_ERR_ARG, "null argument");
+  Server *s = nullptr;
+  int rc = server_create(g, opt, &s);
+  if (rc) return rc;
+  *out = new tdfs_server{s};
+  return TDFS_OK;
+}
+
+int tdfs_server_submit(tdfs_server *s, const tdfs_plan *p, uint64_t *ticket) {
+  if (!s || !p || !ticket) return fail(TDFS_ERR_ARG, "null argument");
+  return server_submit(s->impl, p->dev, ticket);
+}
+
+int tdfs_server_wait(tdfs_server *s, uint64_t ticket, uint64_t *count, double *latency_us) {
+  if (!s) return fail(TDFS_ERR_ARG, "null server");
+  return server_wait(s->impl, ticket, count, latency_us);
+}
+
+int tdfs_server_stats(tdfs_server *s, tdfs_serve_stats *st) {
+  if (!s || !st) return fail(TDFS_ERR_ARG, "null argument");
+  return server_stats(s->impl, st);
+}
+
+int tdfs_server_destroy(tdfs_server *s) {
+  if (!s) return TDFS_OK;
+  const int rc = server_destroy(s->impl);
+  delete s;
+  return rc;
 }
 
 }  // extern "C"

@@ -404,9 +404,11 @@ struct Engine {
   __device__ void load_plan(int s) {
     if (W.slot == s) return;
     __syncwarp();
+    // the host may have written this slot while the kernel runs (serving):
+    // read it through L2 (ld.cg), never from a stale L1 line
     const int32_t *srcw = reinterpret_cast<const int32_t *>(&tab->plan[s]);
     int32_t *dstw = reinterpret_cast<int32_t *>(&W.plan);
-    for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dstw[t] = srcw[t];
+    for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dstw[t] = __ldcg(srcw + t);
     if (lane == 0) W.slot = s;
     __syncwarp();
   }
@@ -424,7 +426,8 @@ struct Engine {
     const int old = atomicSub(&h.holders, 1);
     if (old == 1) {
       const unsigned long long t = *(volatile unsigned long long *)&h.ticket;
-      if ((long long)t >= tab->info[s].ntickets && atomicCAS(&h.state, kSlotActive, kSlotDone) == kSlotActive) {
+      if ((long long)t >= __ldcg(&tab->info[s].ntickets) &&
+          atomicCAS(&h.state, kSlotActive, kSlotDone) == kSlotActive) {
         h.t_done = now_ns();
         __threadfence();
         atomicAdd(&tab->ctl.completed, 1ull);
@@ -437,9 +440,9 @@ struct Engine {
   // phi(1)).  Returns false when no edge of the chunk passes the filter.
   __device__ bool fetch_chunk(int s, long long t) {
     const SlotInfo &in = tab->info[s];
-    const int64_t e0 = in.e_begin + (t * in.stride + in.phase) * (int64_t)kEdgeChunk;
+    const int64_t e0 = __ldcg(&in.e_begin) + (t * __ldcg(&in.stride) + __ldcg(&in.phase)) * (int64_t)kEdgeChunk;
     const int64_t e = e0 + lane;
-    bool ok = e < in.e_end;
+    bool ok = e < __ldcg(&in.e_end);
     int32_t r = 0, c = 0;
     if (ok) {
       r = G.src[e];
@@ -476,7 +479,7 @@ struct Engine {
         unsigned long long lo = *(volatile unsigned long long *)&C.first_open;
         for (unsigned long long q = lo; q < adm && s < 0; ++q) {
           SlotHot &h = tab->hot[q];
-          const long long nt = tab->info[q].ntickets;
+          const long long nt = __ldcg(&tab->info[q].ntickets);
           if ((long long)*(volatile unsigned long long *)&h.ticket >= nt) {
             if (q == lo) {  // advance the hint past exhausted slots
               atomicMax(&C.first_open, q + 1);
@@ -505,7 +508,7 @@ struct Engine {
         long long nt = 0;
         if (lane == 0) {
           const unsigned long long tk = atomicAdd(&tab->hot[s].ticket, 1ull);
-          nt = (long long)tk < tab->info[s].ntickets ? (long long)tk : -1;
+          nt = (long long)tk < __ldcg(&tab->info[s].ntickets) ? (long long)tk : -1;
           if (nt < 0) release_lane0(s);
         }
         nt = __shfl_sync(kFull, nt, 0);

@@ -1,0 +1,29 @@
+// serve.h -- continuous-batching query server (serve.cpp).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "common.h"
+#include "graph.h"
+#include "match.cuh"
+
+namespace tdfs {
+
+// Launch shape of the persistent match kernel (capi.cpp).
+struct LaunchShape {
+  int warps_per_block;
+  int blocks;
+  KernelCfg cfg;
+};
+int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out);
+
+struct Server;
+size_t query_bytes(int k, int cap, int warps_per_block);
+int server_create(tdfs_graph *g, const tdfs_server_options *o, Server **out);
+int server_submit(Server *s, const DevPlan &plan, uint64_t *ticket);
+int server_wait(Server *s, uint64_t ticket, uint64_t *count, double *latency_us);
+int server_stats(Server *s, tdfs_serve_stats *st);
+int server_destroy(Server *s);
+
+}  // namespace tdfs
