@@ -49,6 +49,12 @@ typedef struct {
   int edge_stride;      /* level-0 chunks are dealt round-robin over edge_stride */
   int edge_phase;       /*   shards; this call takes chunks == edge_phase (mod) */
   void *stream;         /* cudaStream_t; NULL = legacy default stream */
+  int steal_min;        /* steal / donate only levels with >= steal_min items left (0 auto = 2) */
+  int merge_ratio;      /* merge a list whose length <= merge_ratio x the scanned span, else
+                           search it (0 auto = 4) */
+  int graph_capture;    /* 1: launch through a cached CUDA graph (upload, reset, kernel,
+                           read-back captured once per launch shape and batch size) */
+  int pad_;
 } tdfs_options;
 
 const char *tdfs_last_error(void);
@@ -92,6 +98,16 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
  * All plans run in one persistent launch; counts[i] belongs to plans[i]. */
 int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
                      const tdfs_options *opt, uint64_t *counts, float *kernel_ms);
+
+/* ---- autotuner (no reference counterpart; the reference's shape is fixed at
+ *      compile time, src/config.h:15-27) ---------------------------------------
+ * Times launch shapes on a sample of the batch (the level-0 chunks t with
+ * t % sample_stride == 0) by coordinate descent over warps per CTA, candidate
+ * chunk depth, the steal threshold, stealing on/off, the merge window and the
+ * merge/search switch point, and returns the fastest as *best (base's edge
+ * range and stream kept).  *best_ms = its sample time. */
+int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *base,
+                  int sample_stride, tdfs_options *best, float *best_ms);
 
 /* ---- serving (no reference counterpart; the north-star served stream) -----
  * A continuous-batching server over one device-resident graph: queries

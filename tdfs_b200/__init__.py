@@ -36,7 +36,7 @@ EXPORTS = [
     "tdfs_count", "tdfs_count_batch",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
     "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern",
-    "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
+    "tdfs_autotune", "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
     "tdfs_server_stats", "tdfs_server_destroy",
 ]
 
@@ -60,6 +60,10 @@ class Options(C.Structure):
         ("edge_stride", C.c_int),
         ("edge_phase", C.c_int),
         ("stream", C.c_void_p),
+        ("steal_min", C.c_int),
+        ("merge_ratio", C.c_int),
+        ("graph_capture", C.c_int),
+        ("pad_", C.c_int),
     ]
 
 
@@ -126,6 +130,8 @@ def lib() -> C.CDLL:
     L.tdfs_gen_chung_lu.argtypes = [i64, i64, C.c_double, i32, C.c_uint64, pp]
     L.tdfs_gen_rmat.argtypes = [ci, ci, C.c_double, C.c_double, C.c_double, C.c_uint64, pp]
     L.tdfs_gen_pattern.argtypes = [ci, C.c_double, ci, C.c_uint64, C.c_char_p, C.c_size_t]
+    L.tdfs_autotune.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), ci, C.POINTER(Options),
+                                C.POINTER(C.c_float)]
     L.tdfs_server_options_default.argtypes = [C.POINTER(ServerOptions)]
     L.tdfs_server_options_default.restype = None
     L.tdfs_server_create.argtypes = [vp, C.POINTER(ServerOptions), pp]
@@ -331,6 +337,17 @@ def shard_edge_ranges(nedges: int, rank: int, world: int):
             return out
         out.append((b, min(nedges, b + EDGE_CHUNK)))
         t += 1
+
+
+def autotune(graph: GraphPreprocessor, patterns, base: Options | None = None, sample_stride: int = 16):
+    """Fastest launch options for this graph and batch of patterns, timed on
+    every sample_stride-th level-0 chunk.  Returns (Options, sample ms)."""
+    arr = (C.c_void_p * len(patterns))(*[p._h.value for p in patterns])
+    best = Options()
+    ms = C.c_float()
+    _check(lib().tdfs_autotune(graph._h, arr, len(patterns), None if base is None else C.byref(base), sample_stride,
+                               C.byref(best), C.byref(ms)))
+    return best, ms.value
 
 
 class Server:

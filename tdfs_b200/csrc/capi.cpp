@@ -82,6 +82,9 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.warp_bytes = (int)((warp_smem_bytes(kmax, cap, window) + 15) & ~(size_t)15);
   c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
   c.idle_ms = 30000;
+  c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
+  c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
+  if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
   const size_t smem = (size_t)c.warp_bytes * s.warps_per_block;
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
@@ -104,6 +107,107 @@ int64_t ticket_count(int64_t b, int64_t e, int stride, int phase) {
   const int64_t chunks = (e - b + kEdgeChunk - 1) / kEdgeChunk;
   if (chunks <= phase) return 0;
   return (chunks - phase + stride - 1) / stride;
+}
+
+// Captured launches: one CUDA graph per (batch size, mode, launch shape)
+// holding the slot-table upload from the pinned staging copy, the control
+// reset, the kernel and the read-back; replays read the staging copy as it is
+// at replay time.
+struct GraphEntry {
+  int n;
+  bool labeled;
+  int blocks, warps;
+  KernelCfg cfg;
+  cudaGraphExec_t exec;
+};
+
+}  // namespace
+
+void release_graphs(tdfs_graph *g) {
+  if (!g->graphs) return;
+  auto *v = static_cast<std::vector<GraphEntry> *>(g->graphs);
+  for (auto &c : *v) cudaGraphExecDestroy(c.exec);
+  delete v;
+  g->graphs = nullptr;
+}
+
+namespace {
+
+std::vector<GraphEntry> &graph_cache(tdfs_graph *g) {
+  if (!g->graphs) g->graphs = new std::vector<GraphEntry>();
+  return *static_cast<std::vector<GraphEntry> *>(g->graphs);
+}
+
+int enqueue_launch(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, cudaStream_t st) {
+  SlotTable *h = g->htab, *d = g->tab;
+  cudaError_t e = cudaMemcpyAsync(&d->ctl, &h->ctl, sizeof h->ctl, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d->hot, h->hot, sizeof(SlotHot) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d->info, h->info, sizeof(SlotInfo) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d->plan, h->plan, sizeof(DevPlan) * n, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_err(e, "slot table upload");
+  init_launch(g->ctl, queue_hdr(g), st);
+  int rc = launch_match(labeled, graph_view(g), g->ctl, d, g->queue, queue_hdr(g), s.cfg, s.blocks,
+                        s.warps_per_block, st);
+  if (rc) return rc;
+  e = cudaMemcpyAsync(h->hot, d->hot, sizeof(SlotHot) * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(g->hctl, g->ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return cuda_err(e, "read-back");
+  return TDFS_OK;
+}
+
+int collect(tdfs_graph *g, int n, unsigned long long *raw) {
+  const RunCtl &hc = *g->hctl;
+  if (hc.error == TDFS_ERR_TIMEOUT) return fail(TDFS_ERR_TIMEOUT, "a bounded device wait ran out");
+  if (hc.error) return fail(hc.error, "device error %d", hc.error);
+  for (int i = 0; i < n; ++i) {
+    if (g->htab->hot[i].state != kSlotDone) return fail(TDFS_ERR_TIMEOUT, "slot %d did not complete", i);
+    raw[i] = g->htab->hot[i].count;
+  }
+  return TDFS_OK;
+}
+
+int run_captured(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, float *ms, unsigned long long *raw) {
+  cudaError_t e;
+  if (!g->gstream) {
+    cudaStream_t st;
+    e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_err(e, "capture stream");
+    g->gstream = st;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(g->gstream);
+  auto &cache = graph_cache(g);
+  cudaGraphExec_t exec = nullptr;
+  for (auto &c : cache)
+    if (c.n == n && c.labeled == labeled && c.blocks == s.blocks && c.warps == s.warps_per_block &&
+        !std::memcmp(&c.cfg, &s.cfg, sizeof c.cfg))
+      exec = c.exec;
+  if (!exec) {
+    cudaGraph_t graph;
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_err(e, "cudaStreamBeginCapture");
+    int rc = enqueue_launch(g, s, labeled, n, st);
+    e = cudaStreamEndCapture(st, &graph);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_err(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_err(e, "cudaGraphInstantiate");
+    cache.push_back(GraphEntry{n, labeled, s.blocks, s.warps_per_block, s.cfg, exec});
+  }
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  if (ms) {
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, st);
+  }
+  e = cudaGraphLaunch(exec, st);
+  if (ms) cudaEventRecord(ev1, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && ms) e = cudaEventElapsedTime(ms, ev0, ev1);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  if (e != cudaSuccess) return cuda_err(e, "graph launch");
+  return collect(g, n, raw);
 }
 
 // One launch over n plans of the same mode: slot i counts plans[i] on the
@@ -144,6 +248,7 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
     if (in.ntickets == 0) ++h->ctl.completed;
     h->plan[i] = *plans[i];
   }
+  if (o.graph_capture) return run_captured(g, s, labeled, n, ms, raw);
   cudaStream_t st = static_cast<cudaStream_t>(o.stream);
   SlotTable *d = g->tab;
   e = cudaMemcpyAsync(&d->ctl, &h->ctl, sizeof h->ctl, cudaMemcpyHostToDevice, st);
@@ -325,6 +430,71 @@ int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, c
     }
   }
   if (kernel_ms) *kernel_ms = total;
+  return TDFS_OK;
+}
+
+int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *base,
+                  int sample_stride, tdfs_options *best, float *best_ms) {
+  if (!g || !plans || nplans <= 0 || !best) return fail(TDFS_ERR_ARG, "bad arguments");
+  tdfs_options b;
+  if (base) b = *base; else tdfs_options_default(&b);
+  if (sample_stride < 1) sample_stride = 1;
+  // resolve the automatic values so every knob has a concrete start
+  tdfs_options cur = b;
+  int kmax = 3;
+  for (int i = 0; i < nplans; ++i) kmax = std::max(kmax, plans[i]->host.k);
+  if (cur.warps_per_block <= 0) cur.warps_per_block = 8;
+  if (cur.chunk_cap <= 0) cur.chunk_cap = kmax >= 6 ? 256 : 512;
+  if (cur.merge_window == 0) cur.merge_window = 128;
+  if (cur.steal < 0) cur.steal = 1;
+  if (cur.steal_min <= 0) cur.steal_min = 2;
+  if (cur.merge_ratio <= 0) cur.merge_ratio = 4;
+  cur.edge_stride = sample_stride;
+  cur.edge_phase = 0;
+  std::vector<uint64_t> counts(nplans);
+  auto measure = [&](const tdfs_options &o, float *out) -> int {
+    float bestt = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      float ms = 0.f;
+      int rc = tdfs_count_batch(g, plans, nplans, &o, counts.data(), &ms);
+      if (rc) return rc;
+      bestt = std::min(bestt, ms);
+    }
+    *out = bestt;
+    return TDFS_OK;
+  };
+  float cur_ms = 0.f;
+  int rc = measure(cur, &cur_ms);
+  if (rc) return rc;
+  struct Knob {
+    int tdfs_options::*field;
+    std::vector<int> values;
+  };
+  const std::vector<Knob> knobs = {
+      {&tdfs_options::warps_per_block, {4, 8}},
+      {&tdfs_options::chunk_cap, {128, 256, 512, 1024}},
+      {&tdfs_options::merge_window, {-1, 128, 256}},
+      {&tdfs_options::merge_ratio, {1, 4, 16}},
+      {&tdfs_options::steal, {0, 1}},
+      {&tdfs_options::steal_min, {2, 8, 32}},
+  };
+  for (const Knob &k : knobs) {
+    for (int v : k.values) {
+      if (cur.*(k.field) == v) continue;
+      tdfs_options t = cur;
+      t.*(k.field) = v;
+      float ms = 0.f;
+      if (measure(t, &ms)) continue;  // a shape that does not fit is skipped
+      if (ms < cur_ms * 0.97f) {
+        cur = t;
+        cur_ms = ms;
+      }
+    }
+  }
+  cur.edge_stride = b.edge_stride;
+  cur.edge_phase = b.edge_phase;
+  *best = cur;
+  if (best_ms) *best_ms = cur_ms;
   return TDFS_OK;
 }
 

@@ -86,6 +86,8 @@ void release(tdfs_graph *g) {
   cudaFree(g->queue);
   cudaFree(g->tab);
   if (g->htab) cudaFreeHost(g->htab);
+  if (g->hctl) cudaFreeHost(g->hctl);
+  g->hctl = nullptr;
   g->tab = nullptr;
   g->htab = nullptr;
   g->rowptr = nullptr;
@@ -124,6 +126,7 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   CK(cudaMalloc(&g->queue, sizeof(SplitUnit) * kQueueCap + sizeof(QueueHdr)));
   CK(cudaMalloc(&g->tab, sizeof(SlotTable)));
   CK(cudaMallocHost(&g->htab, sizeof(SlotTable)));
+  CK(cudaMallocHost(&g->hctl, sizeof(RunCtl)));
   CK(cudaMemcpy(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(g->colidx, colidx, sizeof(int32_t) * nedges, cudaMemcpyHostToDevice));
   CK(cudaMemset(g->colidx + nedges, 0x7f, sizeof(int32_t) * kColPad));
@@ -164,6 +167,9 @@ void graph_release(tdfs_graph *g) {
   int cur = 0;
   cudaGetDevice(&cur);
   cudaSetDevice(g->device);
+  release_graphs(g);
+  if (g->gstream) cudaStreamDestroy(static_cast<cudaStream_t>(g->gstream));
+  g->gstream = nullptr;
   release(g);
   cudaSetDevice(cur);
   delete g;

@@ -98,6 +98,9 @@ struct tdfs_graph {
   tdfs::SplitUnit *queue; // split-unit ring: kQueueCap units then a QueueHdr
   tdfs::SlotTable *tab;   // query slots of a launch
   tdfs::SlotTable *htab;  // pinned host staging copy of the slot table
+  tdfs::RunCtl *hctl;     // pinned host copy of the control block
+  void *gstream;          // cudaStream_t for captured launches (created on first use)
+  void *graphs;           // cache of instantiated launch graphs (capi.cpp)
   size_t bytes;
 };
 
@@ -106,6 +109,7 @@ namespace tdfs {
 int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx, const int32_t *labels,
                  int device, int32_t max_degree, tdfs_graph **out);
 void graph_release(tdfs_graph *g);
+void release_graphs(tdfs_graph *g);  // capi.cpp: destroys cached launch graphs
 DevGraph graph_view(const tdfs_graph *g);
 inline QueueHdr *queue_hdr(tdfs_graph *g) { return reinterpret_cast<QueueHdr *>(g->queue + kQueueCap); }
 

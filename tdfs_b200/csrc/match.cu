@@ -266,7 +266,7 @@ struct Engine {
     if (!LAB && lo >= 0 && slen > 0 && (slen > 64 || closed)) spos = warp_upper_bound(src, 0, slen, lo);
     // merge (staged window) or per-lane search, per list, by degree ratio
     uint32_t mm = 0;
-    if (cfg.window > 0 && myslot >= 0 && (int64_t)mylen <= 4ll * max(1, slen - spos)) mm = 1u << myslot;
+    if (cfg.window > 0 && myslot >= 0 && (int64_t)mylen <= (int64_t)cfg.merge_ratio * max(1, slen - spos)) mm = 1u << myslot;
     mm = __reduce_or_sync(kFull, mm);
     if (lane == 0) {
       H.src = src;
@@ -569,7 +569,7 @@ struct Engine {
         const unsigned long long o = __shfl_xor_sync(kFull, key, s);
         key = o > key ? o : key;
       }
-      if ((int)(key >> 32) < 2) continue;
+      if ((int)(key >> 32) < cfg.steal_min) continue;
       vic = (int)(key & 0xffffffffu) - 1;
       WarpSmem &V = warp_at(vic);
       unsigned long long w = 0;
@@ -577,7 +577,7 @@ struct Engine {
       w = __shfl_sync(kFull, w, 0);
       __threadfence_block();
       const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
-      if (n - it < 2) continue;
+      if (n - it < cfg.steal_min) continue;
       const int vslot = *(volatile int32_t *)&V.slot;
       if (vslot < 0) continue;
       const int take = (n - it) / 2;

@@ -50,6 +50,8 @@ struct KernelCfg {
   int32_t steal;        // 1: stealing + donation on
   int32_t window;       // merge window in ints (multiple of 128) or 0 = off
   int32_t idle_ms;      // bounded idle wait before a warp reports a timeout
+  int32_t steal_min;    // a thief takes half of a level only when >= steal_min items remain
+  int32_t merge_ratio;  // merge a list when its length <= merge_ratio x the source span
   int32_t pad_;
 };
 

@@ -194,3 +194,20 @@ def test_batch_on_edge_ranges(cl, T):
              for b in range(0, e, e // 3 + 1)]
     whole, _ = T.count_batch(cl.dev, plans)
     assert [sum(p[i] for p in parts) for i in range(3)] == whole
+
+
+def test_captured_launch_and_autotuned_options(cl, T):
+    """Launches replayed from a cached CUDA graph, and the autotuner's chosen
+    options, both give the counts of the default launch."""
+    rng = random.Random(17)
+    plans = [T.PatternPreprocessor(text=t) for t in (TRIANGLE, CYCLE4, clique(4), HOUSE)]
+    plans += [T.PatternPreprocessor(text=random_pattern(4 + t % 3, 0.5, 4, rng), labeled=True) for t in range(4)]
+    want, _ = T.count_batch(cl.dev, plans)
+    for _ in range(3):  # the first call captures, the others replay
+        got, _ = T.count_batch(cl.dev, plans, T.default_options(graph_capture=1))
+        assert got == want
+    best, ms = T.autotune(cl.dev, plans, sample_stride=8)
+    assert ms > 0 and best.edge_stride == 1
+    assert T.count_batch(cl.dev, plans, best)[0] == want
+    best.graph_capture = 1
+    assert T.count_batch(cl.dev, plans, best)[0] == want
