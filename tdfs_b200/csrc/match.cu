@@ -806,7 +806,9 @@ struct Engine {
           continue;
         }
         // ---- idle: retire when every admitted slot is done and no more will
-        // come; otherwise wait (bounded) for splits or admissions
+        // come, or -- without stealing -- as soon as admissions are closed and
+        // no tickets are left (nothing else could reach this warp); otherwise
+        // wait (bounded) for splits or admissions
         int done = 0;
         if (lane == 0) {
           if (!hungry && cfg.steal) atomicAdd(&ctl->hungry, 1);
@@ -814,7 +816,7 @@ struct Engine {
           const unsigned long long adm = *(volatile unsigned long long *)&C.admitted;
           const unsigned long long cmp = *(volatile unsigned long long *)&C.completed;
           const int shut = *(volatile int32_t *)&C.shutdown;
-          if (shut && cmp >= adm) done = 1;
+          if (shut && (cmp >= adm || !cfg.steal)) done = 1;
         }
         hungry = cfg.steal != 0;
         done = __shfl_sync(kFull, done, 0);
