@@ -323,12 +323,74 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_serve(args):
+    """Config 5: a stream of random labeled 3-7 vertex queries (density
+    U[0.3, 0.8], labels U[0,4), seed 5) against the labeled power-law graph of
+    config 2 (labels U[0,4), seed 2), arriving as a Poisson process.  Served
+    by the continuous-batching server vs the same queries as sequential plain
+    launches; every served count must equal its plain count."""
+    import random
+    import threading
+    import torch
+    import tdfs_b200 as T
+    torch.cuda.set_device(0)
+    g = T.gen_chung_lu(1_100_000, 3_000_000, 2.1, 30_000, 1).set_labels(4, 2)
+    G = T.GraphPreprocessor(csr=g, labeled=True)
+    rng = random.Random(5)
+    texts = [T.gen_pattern(rng.randint(3, 7), rng.uniform(0.3, 0.8), 4, 5 * 1_000_003 + i) for i in range(args.queries)]
+    qs = [T.PatternPreprocessor(text=t, labeled=True) for t in texts]
+    for q in qs[:8]:
+        T.count(G, q)  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = [T.count(G, q).count for q in qs]
+    t_seq = time.perf_counter() - t0
+    seq_qps = len(qs) / t_seq
+    rate = args.rate if args.rate > 0 else 2.0 * seq_qps
+    srv = T.Server(G, labeled=True, max_inflight=args.inflight)
+    arrivals = []
+    tickets = [None] * len(qs)
+    arr = random.Random(55)
+
+    def producer():
+        t = time.perf_counter()
+        for i, q in enumerate(qs):
+            t += arr.expovariate(rate)
+            d = t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(q)
+
+    th = threading.Thread(target=producer)
+    t1 = time.perf_counter()
+    th.start()
+    th.join()
+    served = [srv.wait(tk) for tk in tickets]
+    t_srv = time.perf_counter() - t1
+    st = srv.stats()
+    srv.close()
+    ok = [c for c, _ in served] == plain
+    return {"metric": "served_queries_per_s", "value": len(qs) / t_srv, "unit": "queries/s", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "ms_per_step": t_srv * 1e3, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic (seeded generators of the benchmark config)",
+            "config": {"workload": f"{len(qs)} random labeled queries (3-7 vertices, density U[0.3,0.8], labels "
+                                   "U[0,4), seed 5) on Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1 with labels "
+                                   f"U[0,4) seed 2; Poisson arrivals at {rate:.1f}/s",
+                       "max_inflight": args.inflight},
+            "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+            "sequential_plain_queries_per_s": seq_qps, "counts_identical_to_plain": ok,
+            "matches_total": sum(plain)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("--queries", type=int, default=400, help="c5: queries in the served stream")
+    ap.add_argument("--rate", type=float, default=0.0, help="c5: Poisson arrival rate (0 = 2x sequential qps)")
+    ap.add_argument("--inflight", type=int, default=256, help="c5: server in-flight limit")
     ap.add_argument("--impl", default="tdfs", choices=["tdfs", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-oracle work for cpu_baseline")
     ap.add_argument("--ref-timeout", type=int, default=600)
@@ -343,6 +405,10 @@ def main():
             import torch
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl" if args.impl == "tdfs" else "gloo", timeout=datetime.timedelta(seconds=900))
+    if args.workload == "c5":
+        if rank == 0:
+            print(json.dumps(run_serve(args)), flush=True)
+        return
     if args.impl == "reference":
         line = run_reference(args, rank, world)
         if rank == 0:
