@@ -180,7 +180,10 @@ def test_batch_equals_single_launches(er, cl, T):
     rng = random.Random(11)
     for case in (er, cl):
         texts = [(TRIANGLE, False), (CYCLE4, False), (clique(4), False), (HOUSE, False), (clique(5), False)]
-        texts += [(random_pattern(3 + t % 5, 0.5, 4, rng), t % 2 == 0) for t in range(12)]
+        # labeled random patterns of every size; unlabeled ones stay small
+        # (a sparse unlabeled 7-vertex pattern has ~1e12 matches here)
+        texts += [(random_pattern(3 + t % 5, 0.5, 4, rng), True) for t in range(10)]
+        texts += [(random_pattern(3 + t % 2, 0.6, 4, rng), False) for t in range(4)]
         plans = [T.PatternPreprocessor(text=t, labeled=lab) for t, lab in texts]
         batch, _ = T.count_batch(case.dev, plans)
         assert batch == [T.count(case.dev, p).count for p in plans]
@@ -196,18 +199,18 @@ def test_batch_on_edge_ranges(cl, T):
     assert [sum(p[i] for p in parts) for i in range(3)] == whole
 
 
-def test_captured_launch_and_autotuned_options(cl, T):
+def test_captured_launch_and_autotuned_options(cl_small, T):
     """Launches replayed from a cached CUDA graph, and the autotuner's chosen
     options, both give the counts of the default launch."""
     rng = random.Random(17)
     plans = [T.PatternPreprocessor(text=t) for t in (TRIANGLE, CYCLE4, clique(4), HOUSE)]
     plans += [T.PatternPreprocessor(text=random_pattern(4 + t % 3, 0.5, 4, rng), labeled=True) for t in range(4)]
-    want, _ = T.count_batch(cl.dev, plans)
+    want, _ = T.count_batch(cl_small.dev, plans)
     for _ in range(3):  # the first call captures, the others replay
-        got, _ = T.count_batch(cl.dev, plans, T.default_options(graph_capture=1))
+        got, _ = T.count_batch(cl_small.dev, plans, T.default_options(graph_capture=1))
         assert got == want
-    best, ms = T.autotune(cl.dev, plans, sample_stride=8)
+    best, ms = T.autotune(cl_small.dev, plans, sample_stride=8)
     assert ms > 0 and best.edge_stride == 1
-    assert T.count_batch(cl.dev, plans, best)[0] == want
+    assert T.count_batch(cl_small.dev, plans, best)[0] == want
     best.graph_capture = 1
-    assert T.count_batch(cl.dev, plans, best)[0] == want
+    assert T.count_batch(cl_small.dev, plans, best)[0] == want

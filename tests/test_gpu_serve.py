@@ -19,10 +19,12 @@ def graph(T):
 
 
 def _queries(T, n, seed, labeled):
+    """Random connected queries; labeled ones of 3-7 vertices, unlabeled ones
+    of 3-5 (larger sparse unlabeled patterns have ~1e10+ matches here)."""
     rng = random.Random(seed)
     out = []
     for i in range(n):
-        k = 3 + rng.randrange(5)
+        k = 3 + rng.randrange(5 if labeled else 3)
         out.append(T.PatternPreprocessor(text=random_pattern(k, rng.uniform(0.3, 0.8), 4, rng), labeled=labeled))
     return out
 
