@@ -54,7 +54,8 @@ typedef struct {
                            search it (0 auto = 4) */
   int graph_capture;    /* 1: launch through a cached CUDA graph (upload, reset, kernel,
                            read-back captured once per launch shape and batch size) */
-  int pad_;
+  int edge_chunk;       /* directed edges per level-0 ticket: 8, 16, 32 (0 auto; 32 whenever
+                           edge_stride > 1, the chunk the round-robin dealing is defined on) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

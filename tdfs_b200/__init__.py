@@ -63,7 +63,7 @@ class Options(C.Structure):
         ("steal_min", C.c_int),
         ("merge_ratio", C.c_int),
         ("graph_capture", C.c_int),
-        ("pad_", C.c_int),
+        ("edge_chunk", C.c_int),
     ]
 
 

@@ -85,6 +85,8 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
+  if (o.edge_chunk != 0 && o.edge_chunk != 8 && o.edge_chunk != 16 && o.edge_chunk != 32)
+    return fail(TDFS_ERR_ARG, "edge_chunk must be 0, 8, 16 or 32");
   const size_t smem = (size_t)c.warp_bytes * s.warps_per_block;
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
@@ -102,9 +104,9 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
 namespace {
 
 // Level-0 tickets of an edge range dealt round-robin: ticket t covers the
-// chunk of 32 edges starting at e_begin + (t * stride + phase) * 32.
-int64_t ticket_count(int64_t b, int64_t e, int stride, int phase) {
-  const int64_t chunks = (e - b + kEdgeChunk - 1) / kEdgeChunk;
+// chunk of `chunk` edges starting at e_begin + (t * stride + phase) * chunk.
+int64_t ticket_count(int64_t b, int64_t e, int stride, int phase, int chunk) {
+  const int64_t chunks = (e - b + chunk - 1) / chunk;
   if (chunks <= phase) return 0;
   return (chunks - phase + stride - 1) / stride;
 }
@@ -236,13 +238,15 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   std::memset(&h->ctl, 0, sizeof h->ctl);
   h->ctl.admitted = (unsigned long long)n;
   h->ctl.shutdown = 1;
+  const int chunk = auto_chunk(std::max<int64_t>(0, ee - eb), stride, s.blocks * s.warps_per_block, o.edge_chunk);
   for (int i = 0; i < n; ++i) {
     SlotInfo &in = h->info[i];
     in.e_begin = eb;
     in.e_end = std::max(eb, ee);
     in.stride = stride;
     in.phase = o.edge_phase;
-    in.ntickets = ticket_count(in.e_begin, in.e_end, stride, o.edge_phase);
+    in.chunk = chunk;
+    in.ntickets = ticket_count(in.e_begin, in.e_end, stride, o.edge_phase, chunk);
     std::memset(&h->hot[i], 0, sizeof h->hot[i]);
     h->hot[i].state = in.ntickets > 0 ? kSlotActive : kSlotDone;  // an empty range is done at once
     if (in.ntickets == 0) ++h->ctl.completed;
@@ -477,6 +481,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::merge_ratio, {1, 4, 16}},
       {&tdfs_options::steal, {0, 1}},
       {&tdfs_options::steal_min, {2, 8, 32}},
+      {&tdfs_options::edge_chunk, {8, 16, 32}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {

@@ -60,6 +60,8 @@ struct SlotInfo {
   int64_t e_end;
   int64_t ntickets;  // tickets of this slot
   int32_t stride, phase;
+  int32_t chunk;     // directed edges per ticket (8, 16 or 32)
+  int32_t pad_;
 };
 
 struct alignas(128) SlotCtl {

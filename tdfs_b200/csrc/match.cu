@@ -245,20 +245,28 @@ struct Engine {
         H.mcur[myslot] = 0;
       }
     }
-    int32_t lo = -1, hi = INT_MAX, nneq = 0;
-    int32_t neq[kMaxK];
-#pragma unroll
-    for (int j = 0; j < kMaxK; ++j) {
-      if (j >= i) break;
-      const int32_t v = W.phi[j];
+    // bounds from the symmetry conditions; the excluded vertices are packed
+    // into shared memory by ballot (lane j looks at phi(j))
+    int32_t lo = -1, hi = INT_MAX;
+    bool isneq = false;
+    int32_t myphi = 0;
+    if (lane < i) {
+      myphi = W.phi[lane];
       if (LAB) {
-        neq[nneq++] = v;
+        isneq = true;
+      } else if (P.larger[i] >> lane & 1) {
+        lo = myphi;
+      } else if (P.less[i] >> lane & 1) {
+        hi = myphi;
       } else {
-        if (P.larger[i] >> j & 1) lo = max(lo, v);
-        else if (P.less[i] >> j & 1) hi = min(hi, v);
-        else neq[nneq++] = v;
+        isneq = true;
       }
     }
+    lo = __reduce_max_sync(kFull, (unsigned)(lo + 1)) - 1;  // lo >= -1
+    hi = (int32_t)__reduce_min_sync(kFull, (unsigned)hi);
+    const unsigned nmask = __ballot_sync(kFull, isneq);
+    const int nneq = __popc(nmask);
+    if (isneq) H.neqv[__popc(nmask & lanemask_lt())] = myphi;
     // skip the prefix <= lo by a 32-ary search; a short source is cheaper to
     // filter in the scan, except when the closed-form count needs the bound
     int32_t spos = 0;
@@ -276,7 +284,6 @@ struct Engine {
       H.hi = hi;
       H.nm = nm;
       H.nneq = nneq;
-      for (int t = 0; t < kMaxK; ++t) H.neqv[t] = t < nneq ? neq[t] : -1;
       H.complete = 0;
       H.nprod = -1;
       H.merge_mask = mm;
@@ -314,7 +321,9 @@ struct Engine {
     if (lane == 0) {
       const bool first = H.nprod < 0;
       H.spos = spos;
-      for (int m = 0; m < H.nm; ++m) H.mcur[m] = cur[m];
+#pragma unroll
+      for (int m = 0; m < kMaxLists; ++m)
+        if (m < H.nm) H.mcur[m] = cur[m];
       if (first) {
         H.nprod = n;
         H.complete = spos >= send;
@@ -435,14 +444,16 @@ struct Engine {
     }
   }
 
-  // Level-0 chunk t of slot s: up to 32 directed edges, filtered as get_job
+  // Level-0 chunk t of slot s: up to 32 directed edges (the slot's chunk
+  // size), filtered as get_job
   // (src/gpu_match.cu:531-556), published as level-1 items (pairs phi(0),
   // phi(1)).  Returns false when no edge of the chunk passes the filter.
   __device__ bool fetch_chunk(int s, long long t) {
     const SlotInfo &in = tab->info[s];
-    const int64_t e0 = __ldcg(&in.e_begin) + (t * __ldcg(&in.stride) + __ldcg(&in.phase)) * (int64_t)kEdgeChunk;
+    const int chunk = __ldcg(&in.chunk);
+    const int64_t e0 = __ldcg(&in.e_begin) + (t * __ldcg(&in.stride) + __ldcg(&in.phase)) * (int64_t)chunk;
     const int64_t e = e0 + lane;
-    bool ok = e < __ldcg(&in.e_end);
+    bool ok = lane < chunk && e < __ldcg(&in.e_end);
     int32_t r = 0, c = 0;
     if (ok) {
       r = G.src[e];
@@ -556,70 +567,75 @@ struct Engine {
   // valid iff the CAS succeeds: a warp rewrites its items, prefix, plan or
   // slot only after bumping gen.  Returns the level (1 = edge pairs) or 0.
   __device__ int steal_local(int nwarps, int me) {
-    for (int l = 1; l <= kMaxK - 2; ++l) {
-      int rem = 0, vic = -1;
-      if (lane < nwarps && lane != me) {
-        const unsigned long long w = *(volatile unsigned long long *)&warp_at(lane).word[l];
-        rem = (int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu);
-        vic = lane;
-      }
-      unsigned long long key = ((unsigned long long)(unsigned)max(rem, 0) << 32) | (unsigned)(vic + 1);
-#pragma unroll
-      for (int s = 16; s >= 1; s >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(kFull, key, s);
-        key = o > key ? o : key;
-      }
-      if ((int)(key >> 32) < cfg.steal_min) continue;
-      vic = (int)(key & 0xffffffffu) - 1;
-      WarpSmem &V = warp_at(vic);
-      unsigned long long w = 0;
-      if (lane == 0) w = *(volatile unsigned long long *)&V.word[l];
-      w = __shfl_sync(kFull, w, 0);
-      __threadfence_block();
-      const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
-      if (n - it < cfg.steal_min) continue;
-      const int vslot = *(volatile int32_t *)&V.slot;
-      if (vslot < 0) continue;
-      const int take = (n - it) / 2;
-      const int from = n - take;
-      {  // plan
-        const volatile int32_t *sp = reinterpret_cast<const volatile int32_t *>(&V.plan);
-        int32_t *dp = reinterpret_cast<int32_t *>(&W.plan);
-        for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dp[t] = sp[t];
-      }
-      if (l == 1) {
-        if (lane < take) {
-          W.er[lane] = ((volatile int32_t *)V.er)[from + lane];
-          W.ec[lane] = ((volatile int32_t *)V.ec)[from + lane];
+    // one pass: lane v scans warp v's levels and offers its shallowest level
+    // with at least steal_min items; the warp takes the shallowest offer,
+    // the largest one on ties
+    unsigned long long key = 0;
+    if (lane < nwarps && lane != me) {
+      const WarpSmem &V = warp_at(lane);
+      for (int l = 1; l <= kMaxK - 2; ++l) {
+        const unsigned long long w = *(volatile const unsigned long long *)&V.word[l];
+        const int rem = (int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu);
+        if (rem >= cfg.steal_min) {
+          key = ((unsigned long long)(kMaxK - l) << 40) | ((unsigned long long)rem << 8) | (unsigned)lane;
+          break;
         }
-      } else {
-        const volatile int32_t *vb = buf_of(vic, l);
-        int32_t *mb = buf(l);
-        for (int t = lane; t < take; t += 32) mb[t] = vb[from + t];
-        if (lane < l) W.phi[lane] = ((volatile int32_t *)V.phi)[lane];
-      }
-      __threadfence_block();
-      __syncwarp();
-      int won = 0;
-      if (lane == 0) {
-        atomicAdd(&tab->hot[vslot].holders, 1);
-        won = atomicCAS(&V.word[l], w, (w & ~0xffffull) | (unsigned long long)from) == w;
-        if (won) {
-          W.slot = vslot;
-        } else {
-          release_lane0(vslot);  // nothing to flush: this warp holds no work
-          W.slot = -1;           // the plan copy above overwrote the old one
-        }
-      }
-      won = __shfl_sync(kFull, won, 0);
-      __syncwarp();
-      if (won) {
-        install(l, take);
-        if (lane == 0) atomicAdd(&ctl->steals, 1ull);
-        return l;
       }
     }
-    return 0;
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(kFull, key, s);
+      key = o > key ? o : key;
+    }
+    if (!key) return 0;
+    const int l = kMaxK - (int)(key >> 40);
+    const int vic = (int)(key & 0xff);
+    WarpSmem &V = warp_at(vic);
+    unsigned long long w = 0;
+    if (lane == 0) w = *(volatile unsigned long long *)&V.word[l];
+    w = __shfl_sync(kFull, w, 0);
+    __threadfence_block();
+    const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
+    if (n - it < cfg.steal_min) return 0;
+    const int vslot = *(volatile int32_t *)&V.slot;
+    if (vslot < 0) return 0;
+    const int take = (n - it) / 2;
+    const int from = n - take;
+    {  // plan
+      const volatile int32_t *sp = reinterpret_cast<const volatile int32_t *>(&V.plan);
+      int32_t *dp = reinterpret_cast<int32_t *>(&W.plan);
+      for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dp[t] = sp[t];
+    }
+    if (l == 1) {
+      if (lane < take) {
+        W.er[lane] = ((volatile int32_t *)V.er)[from + lane];
+        W.ec[lane] = ((volatile int32_t *)V.ec)[from + lane];
+      }
+    } else {
+      const volatile int32_t *vb = buf_of(vic, l);
+      int32_t *mb = buf(l);
+      for (int t = lane; t < take; t += 32) mb[t] = vb[from + t];
+      if (lane < l) W.phi[lane] = ((volatile int32_t *)V.phi)[lane];
+    }
+    __threadfence_block();
+    __syncwarp();
+    int won = 0;
+    if (lane == 0) {
+      atomicAdd(&tab->hot[vslot].holders, 1);
+      won = atomicCAS(&V.word[l], w, (w & ~0xffffull) | (unsigned long long)from) == w;
+      if (won) {
+        W.slot = vslot;
+      } else {
+        release_lane0(vslot);  // nothing to flush: this warp holds no work
+        W.slot = -1;           // the plan copy above overwrote the old one
+      }
+    }
+    won = __shfl_sync(kFull, won, 0);
+    __syncwarp();
+    if (!won) return 0;
+    install(l, take);
+    if (lane == 0) atomicAdd(&ctl->steals, 1ull);
+    return l;
   }
 
   // Bounded MPMC ring with per-slot sequence numbers (lane 0 only).  A slot

@@ -55,7 +55,18 @@ struct KernelCfg {
   int32_t pad_;
 };
 
-constexpr int kEdgeChunk = 32;  // directed edges per level-0 ticket
+constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
+
+// Edges per level-0 ticket: 32 when the range is dealt over several shards
+// (the documented round-robin split), else the largest of 32/16/8 that still
+// gives every warp of the grid about two tickets to start with.
+inline int auto_chunk(int64_t edges, int stride, int total_warps, int requested) {
+  if (requested == 8 || requested == 16 || requested == 32) return requested;
+  if (stride > 1) return kEdgeChunk;
+  int c = kEdgeChunk;
+  while (c > 8 && edges / c < 2ll * total_warps) c >>= 1;
+  return c;
+}
 
 size_t warp_smem_bytes(int k, int cap, int window);
 

@@ -162,7 +162,8 @@ int admit(Server &S, std::vector<Pending> &batch) {
     in.e_end = S.g->nedges;
     in.stride = 1;
     in.phase = 0;
-    in.ntickets = (S.g->nedges + kEdgeChunk - 1) / kEdgeChunk;
+    in.chunk = auto_chunk(S.g->nedges, 1, S.shape.blocks * S.shape.warps_per_block, S.opt.launch.edge_chunk);
+    in.ntickets = (S.g->nedges + in.chunk - 1) / in.chunk;
     std::memset(&h->hot[s], 0, sizeof h->hot[s]);
     h->hot[s].state = kSlotActive;
     h->plan[s] = q.plan;
