@@ -56,6 +56,10 @@ typedef struct {
                            read-back captured once per launch shape and batch size) */
   int edge_chunk;       /* directed edges per level-0 ticket: 8, 16, 32 (0 auto; 32 whenever
                            edge_stride > 1, the chunk the round-robin dealing is defined on) */
+  int fixed_stage;      /* last vertex: stage the intersection of its backward neighbours
+                           other than the parent once per parent in shared memory
+                           (0 auto = on, -1 off) */
+  int pad_;
 } tdfs_options;
 
 const char *tdfs_last_error(void);

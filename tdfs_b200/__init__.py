@@ -64,6 +64,8 @@ class Options(C.Structure):
         ("merge_ratio", C.c_int),
         ("graph_capture", C.c_int),
         ("edge_chunk", C.c_int),
+        ("fixed_stage", C.c_int),
+        ("pad_", C.c_int),
     ]
 
 

@@ -79,7 +79,8 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   KernelCfg &c = s.cfg;
   c.cap = cap;
   c.window = window;
-  c.warp_bytes = (int)((warp_smem_bytes(kmax, cap, window) + 15) & ~(size_t)15);
+  c.fixed = o.fixed_stage < 0 ? 0 : 1;
+  c.warp_bytes = (int)((warp_smem_bytes(kmax, cap, window, c.fixed != 0) + 15) & ~(size_t)15);
   c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
   c.idle_ms = 30000;
   c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
@@ -482,6 +483,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::steal, {0, 1}},
       {&tdfs_options::steal_min, {2, 8, 32}},
       {&tdfs_options::edge_chunk, {8, 16, 32}},
+      {&tdfs_options::fixed_stage, {-1, 1}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {

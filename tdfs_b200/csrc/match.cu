@@ -49,6 +49,10 @@ struct alignas(16) WarpSmem {
   int32_t er[kEdgeChunk];        // level-1 items: edge pairs (phi(0), phi(1))
   int32_t ec[kEdgeChunk];
   LevelHdr h[kMaxK];
+  LevelHdr hf;                   // scan of the last vertex's fixed lists
+  int32_t fvalid;                // 0: stale, 1: F holds the fixed set, 2: too large
+  int32_t fn;                    // |F|
+  int32_t pad1_[2];
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -190,13 +194,21 @@ struct Engine {
   }
 
   __device__ __forceinline__ int32_t *buf(int l) { return bufs + (l - 2) * cfg.cap; }
+  __device__ __forceinline__ int32_t *fbuf() { return win + cfg.window; }  // F (cfg.fixed)
   __device__ __forceinline__ int64_t deg(int32_t v) { return G.rowptr[v + 1] - G.rowptr[v]; }
 
   // Set up the candidate scan of pattern vertex i from phi(0..i-1).
   __device__ void setup(int i, bool allow_reuse) {
-    LevelHdr &H = W.h[i];
+    if (i == P.k - 2 && lane == 0) W.fvalid = 0;  // the last vertex's fixed lists change with this parent
+    setup_into(W.h[i], i, allow_reuse, -1);
+  }
+
+  // Set up a scan for vertex i into header H; `excl` >= 0 leaves that earlier
+  // vertex out of the backward neighbours and the conditions (the fixed part
+  // of the last vertex's candidate set, see count_fixed).
+  __device__ void setup_into(LevelHdr &H, int i, bool allow_reuse, int excl) {
     const int dep = P.dep[i];
-    const bool reuse = allow_reuse && dep >= 2 && W.h[dep].complete;
+    const bool reuse = excl < 0 && allow_reuse && dep >= 2 && W.h[dep].complete;
     const int32_t *src;
     int32_t slen;
     int nm = 0;
@@ -218,9 +230,11 @@ struct Engine {
       // scan the smallest backward-neighbour list (first on ties, as
       // src/gpu_match.cu:646-663)
       const int nbn = P.nbn[i];
+      const bool part = lane < nbn && P.bn[i][lane] != excl;
+      const unsigned pmask = __ballot_sync(kFull, part);
       unsigned long long key = ~0ull;
       int64_t b = 0, e = 0;
-      if (lane < nbn) {
+      if (part) {
         const int32_t v = W.phi[P.bn[i][lane]];
         b = G.rowptr[v];
         e = G.rowptr[v + 1];
@@ -236,9 +250,11 @@ struct Engine {
       const int64_t sb = __shfl_sync(kFull, b, bmin);
       slen = (int32_t)(best >> 8);
       src = G.colidx + sb;
-      nm = nbn - 1;
-      if (lane < nbn && lane != bmin) {
-        myslot = lane < bmin ? lane : lane - 1;
+      nm = __popc(pmask) - 1;
+      if (part && lane != bmin) {
+        const int rank = __popc(pmask & lanemask_lt());
+        const int rmin = __popc(pmask & ((1u << bmin) - 1u));
+        myslot = rank < rmin ? rank : rank - 1;
         mylen = (int32_t)(e - b);
         H.mlist[myslot] = G.colidx + b;
         H.mlen[myslot] = mylen;
@@ -250,7 +266,7 @@ struct Engine {
     int32_t lo = -1, hi = INT_MAX;
     bool isneq = false;
     int32_t myphi = 0;
-    if (lane < i) {
+    if (lane < i && lane != excl) {
       myphi = W.phi[lane];
       if (LAB) {
         isneq = true;
@@ -270,7 +286,7 @@ struct Engine {
     // skip the prefix <= lo by a 32-ary search; a short source is cheaper to
     // filter in the scan, except when the closed-form count needs the bound
     int32_t spos = 0;
-    const bool closed = !LAB && nm == 0 && hi == INT_MAX && i == P.k - 1;
+    const bool closed = !LAB && nm == 0 && hi == INT_MAX && i == P.k - 1 && excl < 0;
     if (!LAB && lo >= 0 && slen > 0 && (slen > 64 || closed)) spos = warp_upper_bound(src, 0, slen, lo);
     // merge (staged window) or per-lane search, per list, by degree ratio
     uint32_t mm = 0;
@@ -338,7 +354,121 @@ struct Engine {
   }
 
   // Count the candidates of the last pattern vertex (not stored).
+  // The last vertex's backward neighbours other than its parent (vertex i-1)
+  // are the same for every sibling at level i-1: their filtered intersection
+  // F is built once per parent into shared memory, and each sibling then
+  // counts |F ∩ N(phi(i-1))| under the one condition that involves the
+  // parent.  Applies when the parent is a backward neighbour, at least one
+  // other backward neighbour exists and the plan does not reuse a level.
+  __device__ bool fixed_applies(int i) {
+    if (!cfg.fixed || i < 3 || P.dep[i] >= 0 || P.nbn[i] < 2) return false;
+    bool has_parent = false;
+    for (int t = 0; t < P.nbn[i]; ++t) has_parent |= P.bn[i][t] == i - 1;
+    return has_parent;
+  }
+
+  __device__ void build_fixed(int i) {
+    LevelHdr &H = W.hf;
+    setup_into(H, i, false, i - 1);
+    int32_t *out = fbuf();
+    const int32_t *src = H.src;
+    const int32_t send = H.send;
+    int32_t cur[kMaxLists];
+#pragma unroll
+    for (int m = 0; m < kMaxLists; ++m) cur[m] = m < H.nm ? H.mcur[m] : 0;
+    int32_t n = 0;
+    bool over = false;
+    for (int32_t spos = H.spos; spos < send; spos += 32) {
+      if (n > cfg.cap - 32) {  // a full step could write past the buffer: give up
+        over = true;
+        break;
+      }
+      const int32_t idx = spos + lane;
+      const bool valid = idx < send;
+      const int32_t x = valid ? src[idx] : 0;
+      bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
+      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx, false, Window{0, 0});
+      const unsigned mask = __ballot_sync(kFull, ok);
+      if (ok) out[n + __popc(mask & lanemask_lt())] = x;
+      n += __popc(mask);
+    }
+    __syncwarp();
+    if (lane == 0) {
+      W.fn = n;
+      W.fvalid = over ? 2 : 1;
+    }
+    __syncwarp();
+  }
+
+  __device__ unsigned long long count_fixed(int i) {
+    const int par = i - 1;
+    const int32_t x = W.phi[par];
+    const int32_t *F = fbuf();
+    const int32_t nF = W.fn;
+    if (nF == 0) return 0;
+    int64_t b = 0, e = 0;
+    if (lane == 0) {
+      b = G.rowptr[x];
+      e = G.rowptr[x + 1];
+    }
+    b = __shfl_sync(kFull, b, 0);
+    e = __shfl_sync(kFull, e, 0);
+    const int32_t *L = G.colidx + b;
+    const int32_t len = (int32_t)(e - b);
+    // the condition between the last vertex y and its parent x
+    const int rel = LAB ? 0 : (P.larger[i] >> par & 1) ? 1 : (P.less[i] >> par & 1) ? 2 : 0;
+    unsigned long long c = 0;
+    if ((int64_t)len <= 4ll * nF) {
+      // scan N(x) (coalesced), look each y up in F (shared memory)
+      int32_t start = 0;
+      if (rel == 1 && len > 64) start = warp_upper_bound(L, 0, len, x);
+      for (int32_t pos = start; pos < len; pos += 32) {
+        const int32_t idx = pos + lane;
+        const bool valid = idx < len;
+        const int32_t y = valid ? L[idx] : 0;
+        bool ok = valid && (rel == 1 ? y > x : rel == 2 ? y < x : y != x);
+        if (ok) {
+          const int32_t q = lower_bound(F, 0, nF, y);
+          ok = q < nF && F[q] == y;
+        }
+        c += __popc(__ballot_sync(kFull, ok));
+      }
+    } else {
+      // scan F, search each y in N(x) from a monotone cursor
+      int32_t start = rel == 1 ? upper_bound_smem(F, nF, x) : 0;
+      int32_t curp = 0;
+      for (int32_t pos = start; pos < nF; pos += 32) {
+        const int32_t idx = pos + lane;
+        const bool valid = idx < nF;
+        const int32_t y = valid ? F[idx] : 0;
+        bool ok = valid && (rel == 1 ? y > x : rel == 2 ? y < x : y != x);
+        const bool searched = ok;
+        int32_t p = 0;
+        if (ok) {
+          p = lower_bound(L, curp, len, y);
+          ok = p < len && L[p] == y;
+        }
+        curp = max(curp, (int32_t)__reduce_max_sync(kFull, searched ? (unsigned)p : 0u));
+        c += __popc(__ballot_sync(kFull, ok));
+      }
+    }
+    return c;
+  }
+
+  __device__ __forceinline__ int32_t upper_bound_smem(const int32_t *a, int32_t n, int32_t x) {
+    int32_t lo = 0, hi = n;
+    while (lo < hi) {
+      const int32_t mid = (lo + hi) >> 1;
+      if (a[mid] <= x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+  }
+
   __device__ unsigned long long count_last(int i) {
+    if (fixed_applies(i)) {
+      if (W.fvalid == 0) build_fixed(i);
+      if (W.fvalid == 1) return count_fixed(i);
+    }
     setup(i, true);
     const LevelHdr &H = W.h[i];
     const int32_t *src = H.src;
@@ -471,6 +601,7 @@ struct Engine {
     __syncwarp();
     if (!mask) return false;
     if (lane == 0) {
+      W.fvalid = 0;
       for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
       publish(1, __popc(mask));
     }
@@ -543,6 +674,7 @@ struct Engine {
   }
   __device__ __forceinline__ int32_t *buf_of(int v, int l) {
     return reinterpret_cast<int32_t *>(cta + (size_t)v * cfg.warp_bytes + hdr_bytes) + cfg.window +
+           (cfg.fixed ? cfg.cap : 0) +
            (l - 2) * cfg.cap;
   }
 
@@ -550,6 +682,7 @@ struct Engine {
   // prefix already in W.phi, plan in W.plan) this warp's new base subtree.
   __device__ void install(int l, int cnt) {
     if (lane == 0) {
+      W.fvalid = 0;
       for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
       if (l >= 2) {
         W.h[l].spos = W.h[l].send = 0;  // no source left: only the given candidates
@@ -788,6 +921,7 @@ struct Engine {
       for (int l = 0; l < kStoredMax; ++l) W.word[l] = 0;
       for (int l = 0; l < kMaxK; ++l) W.h[l].complete = 0;
       W.slot = -1;
+      W.fvalid = 0;
     }
     __syncwarp();
     for (;;) {
@@ -914,7 +1048,7 @@ __global__ void __launch_bounds__(256) match_kernel(const __grid_constant__ DevG
   WarpSmem &W = *reinterpret_cast<WarpSmem *>(base);
   const size_t hdr = (sizeof(WarpSmem) + 15) & ~(size_t)15;
   int32_t *win = reinterpret_cast<int32_t *>(base + hdr);
-  int32_t *bufs = win + cfg.window;
+  int32_t *bufs = win + cfg.window + (cfg.fixed ? cfg.cap : 0);
   Engine<LAB> eng(G, cfg, ctl, tab, units, qh, W, bufs, win);
   eng.run(nwarps, me);
 }
@@ -934,10 +1068,10 @@ __global__ void init_kernel(RunCtl *ctl, QueueHdr *qh) {
 
 }  // namespace
 
-size_t warp_smem_bytes(int k, int cap, int window) {
+size_t warp_smem_bytes(int k, int cap, int window, bool fixed) {
   const size_t hdr = (sizeof(WarpSmem) + 15) & ~(size_t)15;
   const int stored = k > 3 ? k - 3 : 0;
-  return hdr + sizeof(int32_t) * ((size_t)window + (size_t)stored * cap);
+  return hdr + sizeof(int32_t) * ((size_t)window + (size_t)(stored + (fixed ? 1 : 0)) * cap);
 }
 
 int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem) {

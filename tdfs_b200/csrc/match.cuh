@@ -52,7 +52,7 @@ struct KernelCfg {
   int32_t idle_ms;      // bounded idle wait before a warp reports a timeout
   int32_t steal_min;    // a thief takes half of a level only when >= steal_min items remain
   int32_t merge_ratio;  // merge a list when its length <= merge_ratio x the source span
-  int32_t pad_;
+  int32_t fixed;        // 1: stage the last vertex's fixed lists once per parent
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
@@ -68,7 +68,7 @@ inline int auto_chunk(int64_t edges, int stride, int total_warps, int requested)
   return c;
 }
 
-size_t warp_smem_bytes(int k, int cap, int window);
+size_t warp_smem_bytes(int k, int cap, int window, bool fixed);
 
 // CTAs of the match kernel that fit on one SM at once (registers, shared
 // memory, threads); -1 on a CUDA error.  The persistent grid must not exceed

@@ -27,6 +27,7 @@ OPTION_SETS = [
     {"merge_window": -1},                            # per-lane search only
     {"chunk_cap": 64, "warps_per_block": 4},         # tiny buffers: many refills
     {"merge_window": 256, "chunk_cap": 128, "blocks_per_sm": 1},
+    {"fixed_stage": -1, "edge_chunk": 32, "steal_min": 8},  # no last-level staging
 ]
 
 
