@@ -59,7 +59,8 @@ typedef struct {
   int fixed_stage;      /* last vertex: stage the intersection of its backward neighbours
                            other than the parent once per parent in shared memory
                            (0 auto = on, -1 off) */
-  int pad_;
+  int split_after_us;   /* a warp's subtree becomes stealable after this many microseconds
+                           on it, donatable to the HBM ring after 4x (0 auto = 5, -1 = at once) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

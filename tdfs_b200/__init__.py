@@ -65,7 +65,7 @@ class Options(C.Structure):
         ("graph_capture", C.c_int),
         ("edge_chunk", C.c_int),
         ("fixed_stage", C.c_int),
-        ("pad_", C.c_int),
+        ("split_after_us", C.c_int),
     ]
 
 

@@ -52,7 +52,7 @@ struct alignas(16) WarpSmem {
   LevelHdr hf;                   // scan of the last vertex's fixed lists
   int32_t fvalid;                // 0: stale, 1: F holds the fixed set, 2: too large
   int32_t fn;                    // |F|
-  int32_t pad1_[2];
+  unsigned long long t_base;     // globaltimer when the current base work was taken
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -602,6 +602,7 @@ struct Engine {
     if (!mask) return false;
     if (lane == 0) {
       W.fvalid = 0;
+      W.t_base = now_ns();
       for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
       publish(1, __popc(mask));
     }
@@ -683,6 +684,7 @@ struct Engine {
   __device__ void install(int l, int cnt) {
     if (lane == 0) {
       W.fvalid = 0;
+      W.t_base = now_ns();
       for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
       if (l >= 2) {
         W.h[l].spos = W.h[l].send = 0;  // no source left: only the given candidates
@@ -704,7 +706,9 @@ struct Engine {
     // with at least steal_min items; the warp takes the shallowest offer,
     // the largest one on ties
     unsigned long long key = 0;
-    if (lane < nwarps && lane != me) {
+    const unsigned long long now = now_ns();
+    if (lane < nwarps && lane != me &&
+        now - *(volatile const unsigned long long *)&warp_at(lane).t_base >= (unsigned long long)cfg.split_after_ns) {
       const WarpSmem &V = warp_at(lane);
       for (int l = 1; l <= kMaxK - 2; ++l) {
         const unsigned long long w = *(volatile const unsigned long long *)&V.word[l];
@@ -870,7 +874,8 @@ struct Engine {
   // shallowest remaining items into the global ring.
   __device__ void maybe_donate(int level) {
     int hungry = 0;
-    if (lane == 0) hungry = *(volatile int32_t *)&ctl->hungry;
+    if (lane == 0 && now_ns() - W.t_base >= 4ull * (unsigned long long)cfg.split_after_ns)
+      hungry = *(volatile int32_t *)&ctl->hungry;
     hungry = __shfl_sync(kFull, hungry, 0);
     if (hungry <= 0) return;
     if (lane == 0) {
@@ -922,6 +927,7 @@ struct Engine {
       for (int l = 0; l < kMaxK; ++l) W.h[l].complete = 0;
       W.slot = -1;
       W.fvalid = 0;
+      W.t_base = 0;
     }
     __syncwarp();
     for (;;) {

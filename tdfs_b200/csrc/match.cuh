@@ -53,6 +53,9 @@ struct KernelCfg {
   int32_t steal_min;    // a thief takes half of a level only when >= steal_min items remain
   int32_t merge_ratio;  // merge a list when its length <= merge_ratio x the source span
   int32_t fixed;        // 1: stage the last vertex's fixed lists once per parent
+  int32_t split_after_ns;  // work becomes stealable after this long on one base subtree
+                           // (donation to the HBM ring after 4x as long)
+  int32_t pad_;
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
