@@ -149,6 +149,21 @@ int tdfs_server_wait(tdfs_server *s, uint64_t ticket, uint64_t *count, double *l
 int tdfs_server_stats(tdfs_server *s, tdfs_serve_stats *st);
 int tdfs_server_destroy(tdfs_server *s); /* drains admitted queries, stops the kernel */
 
+/* ---- counting without device allocation (no counterpart in the reference) --
+ * For callers that cannot call cudaMalloc: a plugin whose host process hands
+ * all device memory to its own allocator, or code that runs where allocating
+ * is not allowed.  Same kernel and counts as tdfs_count; the graph is passed
+ * as device pointers (not checked: the rules of tdfs_graph_from_csr; labels
+ * int32, needed for a labeled pattern) and every working buffer lives in one fixed 48 MiB array inside the
+ * library's device image, held on each GPU that uses the library until the
+ * process exits.  Graphs whose derived arrays do not fit in it are rejected
+ * with TDFS_ERR_CAPACITY (about 4*E + 5*n bytes, up to ~35 MiB, must fit).
+ * The first call on a device looks up the array's address; make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race, so serialise them.  opt may be NULL; opt->stream is honoured. */
+int tdfs_count_static(int device, int64_t n, int64_t nedges, const int64_t *d_rowptr, const int32_t *d_colidx,
+                      const int32_t *d_labels, const tdfs_plan *p, const tdfs_options *opt, uint64_t *count);
+
 /* ---- host CSR: generators and file writer (graph_converter/ output format,
  *      graph_converter/compactify.cpp:172-195, labelize.cpp:130-133) ------- */
 int tdfs_csr_read(const char *prefix, int labeled, tdfs_csr **out);

@@ -36,7 +36,7 @@ EXPORTS = [
     "tdfs_count", "tdfs_count_batch",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
     "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern",
-    "tdfs_autotune", "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
+    "tdfs_autotune", "tdfs_count_static", "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
     "tdfs_server_stats", "tdfs_server_destroy",
 ]
 
@@ -134,6 +134,7 @@ def lib() -> C.CDLL:
     L.tdfs_gen_pattern.argtypes = [ci, C.c_double, ci, C.c_uint64, C.c_char_p, C.c_size_t]
     L.tdfs_autotune.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), ci, C.POINTER(Options),
                                 C.POINTER(C.c_float)]
+    L.tdfs_count_static.argtypes = [ci, i64, i64, vp, vp, vp, vp, C.POINTER(Options), C.POINTER(C.c_uint64)]
     L.tdfs_server_options_default.argtypes = [C.POINTER(ServerOptions)]
     L.tdfs_server_options_default.restype = None
     L.tdfs_server_create.argtypes = [vp, C.POINTER(ServerOptions), pp]
@@ -339,6 +340,17 @@ def shard_edge_ranges(nedges: int, rank: int, world: int):
             return out
         out.append((b, min(nedges, b + EDGE_CHUNK)))
         t += 1
+
+
+def count_static(device: int, n: int, nedges: int, d_rowptr: int, d_colidx: int, d_labels: int | None,
+                 pattern: PatternPreprocessor, options: Options | None = None) -> int:
+    """Count with no device allocation (tdfs_count_static): the graph is
+    given as device pointers, the working memory is the library's fixed
+    per-GPU array."""
+    c = C.c_uint64()
+    _check(lib().tdfs_count_static(device, n, nedges, d_rowptr, d_colidx, d_labels, pattern._h,
+                                   None if options is None else C.byref(options), C.byref(c)))
+    return c.value
 
 
 def autotune(graph: GraphPreprocessor, patterns, base: Options | None = None, sample_stride: int = 16):

@@ -297,6 +297,10 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
 }  // namespace
 }  // namespace tdfs
 
+namespace tdfs {
+const DevPlan &plan_device_table(const tdfs_plan *p) { return p->dev; }
+}  // namespace tdfs
+
 using namespace tdfs;
 
 extern "C" {

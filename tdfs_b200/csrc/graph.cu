@@ -65,6 +65,23 @@ int cuda_fail(cudaError_t e, const char *what) {
 
 }  // namespace
 
+// Derived per-graph arrays into caller-provided device memory, no allocation:
+// edge -> source, neighbour-degree maxima and (when labels is not null) 8-bit
+// labels.  *bad becomes nonzero when a label lies outside [0, 254].
+int prepare_graph_arrays(const int64_t *rowptr, const int32_t *colidx, int32_t n, const int32_t *labels,
+                         int32_t *src, int32_t *maxnd, uint8_t *label8, int32_t *bad, cudaStream_t st) {
+  if (n > 0) {
+    const int threads = 256;
+    const int64_t want = ((int64_t)n * 32 + threads - 1) / threads;
+    const int blocks = (int)std::min<int64_t>(want, 148 * 16);
+    build_src_kernel<<<blocks, threads, 0, st>>>(rowptr, n, src);
+    max_nbr_deg_kernel<<<blocks, threads, 0, st>>>(rowptr, colidx, n, maxnd);
+    if (labels) narrow_labels_kernel<<<148 * 4, 256, 0, st>>>(labels, n, label8, bad);
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? TDFS_OK : cuda_fail(e, "graph preparation kernels");
+}
+
 #define CK(x)                                    \
   do {                                           \
     cudaError_t e_ = (x);                        \

@@ -113,6 +113,8 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
 void graph_release(tdfs_graph *g);
 void release_graphs(tdfs_graph *g);  // capi.cpp: destroys cached launch graphs
 DevGraph graph_view(const tdfs_graph *g);
+int prepare_graph_arrays(const int64_t *rowptr, const int32_t *colidx, int32_t n, const int32_t *labels,
+                         int32_t *src, int32_t *maxnd, uint8_t *label8, int32_t *bad, cudaStream_t st);
 inline QueueHdr *queue_hdr(tdfs_graph *g) { return reinterpret_cast<QueueHdr *>(g->queue + kQueueCap); }
 
 }  // namespace tdfs

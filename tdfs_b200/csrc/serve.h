@@ -18,6 +18,9 @@ struct LaunchShape {
 };
 int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out);
 
+// The device plan table of a compiled pattern (capi.cpp).
+const DevPlan &plan_device_table(const tdfs_plan *p);
+
 struct Server;
 size_t query_bytes(int k, int cap, int warps_per_block);
 int server_create(tdfs_graph *g, const tdfs_server_options *o, Server **out);
