@@ -60,7 +60,7 @@ typedef struct {
                            other than the parent once per parent in shared memory
                            (0 auto = on, -1 off) */
   int split_after_us;   /* a warp's subtree becomes stealable after this many microseconds
-                           on it, donatable to the HBM ring after 4x (0 auto = 5, -1 = at once) */
+                           on it, donatable to the HBM ring after 4x (0 auto = 150, -1 = at once) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);
@@ -185,6 +185,23 @@ int tdfs_gen_rmat(int scale, int edge_factor, double a, double b, double c, uint
 /* random connected pattern in valid matching order (vertex i>0 has an earlier
  * neighbour, vertex 2 is adjacent to vertex 1) written as .g text */
 int tdfs_gen_pattern(int k, double density, int nlabels, uint64_t seed, char *buf, size_t cap);
+
+/* ---- cost estimate before a count (no counterpart in the reference) -------
+ * Knuth's random-probe estimator of the DFS tree the match kernel walks, run
+ * on the host copy of the graph: `probes` random root-to-leaf paths with the
+ * kernel's exact candidate rules (level-0 edge filter, symmetry conditions or
+ * labels, injectivity).  Unbiased for matches and per-depth node counts; the
+ * relative standard errors say how far to trust them.  Used to admit or
+ * schedule queries by expected work; deterministic for a given seed. */
+typedef struct tdfs_estimate_result {
+  double matches;                  /* expected count, as tdfs_count reports it */
+  double nodes[TDFS_MAX_PATTERN];  /* expected partial matches at each depth 1..k-1 */
+  double scanned;                  /* expected adjacency entries the set scans read */
+  double matches_rse;              /* relative standard error of `matches` */
+  double scanned_rse;              /* relative standard error of `scanned` */
+  int64_t probes;
+} tdfs_estimate_result;
+int tdfs_estimate(const tdfs_csr *c, const tdfs_plan *p, int64_t probes, uint64_t seed, tdfs_estimate_result *out);
 
 #ifdef __cplusplus
 }

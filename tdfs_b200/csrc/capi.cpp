@@ -80,7 +80,7 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.cap = cap;
   c.window = window;
   c.fixed = o.fixed_stage < 0 ? 0 : 1;
-  c.split_after_ns = o.split_after_us > 0 ? o.split_after_us * 1000 : (o.split_after_us < 0 ? 0 : 5000);
+  c.split_after_ns = o.split_after_us > 0 ? o.split_after_us * 1000 : (o.split_after_us < 0 ? 0 : 150000);
   c.warp_bytes = (int)((warp_smem_bytes(kmax, cap, window, c.fixed != 0) + 15) & ~(size_t)15);
   c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
   c.idle_ms = 30000;
@@ -489,7 +489,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::steal_min, {2, 8, 32}},
       {&tdfs_options::edge_chunk, {8, 16, 32}},
       {&tdfs_options::fixed_stage, {-1, 1}},
-      {&tdfs_options::split_after_us, {-1, 2, 5, 20, 100}},
+      {&tdfs_options::split_after_us, {-1, 5, 50, 150, 500}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {
