@@ -35,7 +35,7 @@ EXPORTS = [
     "tdfs_plan_compile", "tdfs_plan_from_text", "tdfs_plan_dump", "tdfs_plan_info", "tdfs_plan_free",
     "tdfs_count", "tdfs_count_batch",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
-    "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern",
+    "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern", "tdfs_estimate",
     "tdfs_autotune", "tdfs_count_static", "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
     "tdfs_server_stats", "tdfs_server_destroy",
 ]
@@ -132,6 +132,7 @@ def lib() -> C.CDLL:
     L.tdfs_gen_chung_lu.argtypes = [i64, i64, C.c_double, i32, C.c_uint64, pp]
     L.tdfs_gen_rmat.argtypes = [ci, ci, C.c_double, C.c_double, C.c_double, C.c_uint64, pp]
     L.tdfs_gen_pattern.argtypes = [ci, C.c_double, ci, C.c_uint64, C.c_char_p, C.c_size_t]
+    L.tdfs_estimate.argtypes = [vp, vp, i64, C.c_uint64, vp]
     L.tdfs_autotune.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), ci, C.POINTER(Options),
                                 C.POINTER(C.c_float)]
     L.tdfs_count_static.argtypes = [ci, i64, i64, vp, vp, vp, vp, C.POINTER(Options), C.POINTER(C.c_uint64)]
@@ -215,6 +216,20 @@ def gen_rmat(scale: int, edge_factor: int, a: float, b: float, c: float, seed: i
     h = C.c_void_p()
     _check(lib().tdfs_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(h)))
     return HostCSR(h)
+
+
+class EstimateResult(C.Structure):
+    """Result of tdfs_estimate."""
+    _fields_ = [("matches", C.c_double), ("nodes", C.c_double * 7), ("scanned", C.c_double),
+                ("matches_rse", C.c_double), ("scanned_rse", C.c_double), ("probes", C.c_int64)]
+
+
+def estimate(csr: HostCSR, pattern: "PatternPreprocessor", probes: int = 1000, seed: int = 0) -> EstimateResult:
+    """Expected count and work of a query (tdfs_estimate), from random DFS probes
+    over the host copy of the graph."""
+    r = EstimateResult()
+    _check(lib().tdfs_estimate(csr._h, pattern._h, probes, seed, C.byref(r)))
+    return r
 
 
 def gen_pattern(k: int, density: float, nlabels: int, seed: int) -> str:

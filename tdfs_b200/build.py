@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall", "--expt-relaxed-constexpr"]
 
-SOURCES = ["plan.cpp", "csr.cpp", "capi.cpp", "serve.cpp", "graph.cu", "match.cu", "static_count.cu"]
+SOURCES = ["plan.cpp", "csr.cpp", "capi.cpp", "serve.cpp", "graph.cu", "match.cu", "static_count.cu", "estimate.cpp"]
 HEADERS = ["common.h", "plan.h", "csr.h", "graph.h", "match.cuh", "serve.h"]
 
 

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 #include "common.h"
@@ -13,6 +14,8 @@ struct tdfs_csr {
   std::vector<int32_t> colidx;       // nedges, rows strictly increasing
   std::vector<int32_t> labels;       // n or empty
   int32_t max_degree = 0;
+  // sampling tables of tdfs_estimate (estimate.cpp), built on first use
+  mutable std::shared_ptr<void> estimate_tables;
 };
 
 namespace tdfs {

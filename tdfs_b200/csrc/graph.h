@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda_runtime.h>
 
 #include "common.h"
 
