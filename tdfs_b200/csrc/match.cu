@@ -1028,6 +1028,11 @@ struct Engine {
       if (!idle_since) idle_since = t;
       const SlotCtl &C = tab->ctl;
       const int shut = *(volatile int32_t *)&C.shutdown;
+      // serving: the idle clock runs only while every admitted query is
+      // complete -- a warp that retired while one query was still running
+      // would leave the grid short for the queries admitted after it
+      if (!shut && *(volatile unsigned long long *)&C.completed < *(volatile unsigned long long *)&C.admitted)
+        idle_since = t;
       const unsigned long long limit_ms = shut ? (unsigned long long)cfg.idle_ms : (unsigned long long)C.idle_exit_ms;
       if (t - idle_since > limit_ms * 1000000ull) {
         if (shut) raise_error(ctl, TDFS_ERR_TIMEOUT);
