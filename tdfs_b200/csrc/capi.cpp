@@ -93,11 +93,15 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
                 smem, (size_t)prop.sharedMemPerBlockOptin);
-  const int fit = resident_blocks_per_sm(labeled, s.warps_per_block, smem);
-  if (fit < 0) return fail(TDFS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+  const int fit = resident_blocks_per_sm(labeled, s.warps_per_block, smem, false);
+  const int fit_wide = resident_blocks_per_sm(labeled, s.warps_per_block, smem, true);
+  if (fit < 0 || fit_wide < 0)
+    return fail(TDFS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
   if (fit == 0) return fail(TDFS_ERR_CAPACITY, "the match kernel does not fit on an SM with this shape");
-  // a persistent grid: every CTA resident at once (idle warps wait on busy ones)
+  // a persistent grid: every CTA resident at once (idle warps wait on busy ones);
+  // the 80-register build whenever it holds as many CTAs per SM
   const int per_sm = o.blocks_per_sm > 0 ? std::min(o.blocks_per_sm, fit) : fit;
+  c.wide_regs = per_sm <= fit_wide ? 1 : 0;
   s.blocks = prop.multiProcessorCount * per_sm;
   *out = s;
   return TDFS_OK;

@@ -1048,8 +1048,12 @@ struct Engine {
   }
 };
 
-template <bool LAB>
-__global__ void __launch_bounds__(256) match_kernel(const __grid_constant__ DevGraph G,
+// Two register budgets of one kernel: MINB = 4 CTAs of 256 threads per SM
+// caps it at 64 registers (with a few spills), MINB = 3 gives it 80 and no
+// spills.  A launch whose shared memory already limits it to <= 3 CTAs per
+// SM runs the 80-register build at no cost in occupancy.
+template <bool LAB, int MINB>
+__global__ void __launch_bounds__(256, MINB) match_kernel(const __grid_constant__ DevGraph G,
                                                     const __grid_constant__ KernelCfg cfg, RunCtl *ctl,
                                                     SlotTable *tab, SplitUnit *units, QueueHdr *qh) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1085,18 +1089,24 @@ size_t warp_smem_bytes(int k, int cap, int window, bool fixed) {
   return hdr + sizeof(int32_t) * ((size_t)window + (size_t)(stored + (fixed ? 1 : 0)) * cap);
 }
 
-int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem) {
+namespace {
+
+template <bool LAB, int MINB>
+cudaError_t occupancy(int *n, int warps_per_block, size_t smem) {
+  cudaError_t e = cudaFuncSetAttribute(match_kernel<LAB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, match_kernel<LAB, MINB>, warps_per_block * 32, smem);
+  return e;
+}
+
+}  // namespace
+
+int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem, bool wide) {
   int n = 0;
   cudaError_t e;
-  if (labeled) {
-    e = cudaFuncSetAttribute(match_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, match_kernel<true>, warps_per_block * 32, smem);
-  } else {
-    e = cudaFuncSetAttribute(match_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess)
-      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, match_kernel<false>, warps_per_block * 32, smem);
-  }
+  if (labeled)
+    e = wide ? occupancy<true, 3>(&n, warps_per_block, smem) : occupancy<true, 4>(&n, warps_per_block, smem);
+  else
+    e = wide ? occupancy<false, 3>(&n, warps_per_block, smem) : occupancy<false, 4>(&n, warps_per_block, smem);
   return e == cudaSuccess ? n : -1;
 }
 
@@ -1107,10 +1117,14 @@ void init_launch(RunCtl *ctl, QueueHdr *qh, cudaStream_t stream) {
 int launch_match(bool labeled, const DevGraph &g, RunCtl *ctl, SlotTable *tab, SplitUnit *units, QueueHdr *qh,
                  const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream) {
   const size_t smem = (size_t)cfg.warp_bytes * warps_per_block;
-  if (labeled)
-    match_kernel<true><<<blocks, warps_per_block * 32, smem, stream>>>(g, cfg, ctl, tab, units, qh);
-  else
-    match_kernel<false><<<blocks, warps_per_block * 32, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+  const dim3 grid(blocks), block(warps_per_block * 32);
+  if (labeled) {
+    if (cfg.wide_regs) match_kernel<true, 3><<<grid, block, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+    else match_kernel<true, 4><<<grid, block, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+  } else {
+    if (cfg.wide_regs) match_kernel<false, 3><<<grid, block, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+    else match_kernel<false, 4><<<grid, block, smem, stream>>>(g, cfg, ctl, tab, units, qh);
+  }
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "match kernel launch: %s", cudaGetErrorString(e));
   return TDFS_OK;

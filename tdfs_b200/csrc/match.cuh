@@ -55,7 +55,7 @@ struct KernelCfg {
   int32_t fixed;        // 1: stage the last vertex's fixed lists once per parent
   int32_t split_after_ns;  // work becomes stealable after this long on one base subtree
                            // (donation to the HBM ring after 4x as long)
-  int32_t pad_;
+  int32_t wide_regs;    // 1: the 80-register build (at most 3 CTAs of 256 threads per SM)
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
@@ -74,9 +74,10 @@ inline int auto_chunk(int64_t edges, int stride, int total_warps, int requested)
 size_t warp_smem_bytes(int k, int cap, int window, bool fixed);
 
 // CTAs of the match kernel that fit on one SM at once (registers, shared
-// memory, threads); -1 on a CUDA error.  The persistent grid must not exceed
-// this times the SM count: idle warps wait for busy ones.
-int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem);
+// memory, threads) for its 64-register (wide = false) or 80-register build;
+// -1 on a CUDA error.  The persistent grid must not exceed this times the SM
+// count: idle warps wait for busy ones.
+int resident_blocks_per_sm(bool labeled, int warps_per_block, size_t smem, bool wide);
 
 // Reset the control block and the split ring (stream-ordered).
 void init_launch(RunCtl *ctl, QueueHdr *qh, cudaStream_t stream);
