@@ -159,14 +159,19 @@ def cpu_baseline(g, pats, labeled, rng, budget_s=12.0):
     for name, text in pats:
         P = po.Plan(text, labeled)
         lo, span, byts, cnt, t_pat = b0, 32, 0, 0, 0.0
-        while lo < e0 and t_pat < budget_s / len(pats):
+        share = budget_s / len(pats)
+        while lo < e0 and t_pat < share:
             hi = min(e0, lo + span)
             t0 = time.perf_counter()
             c, nb = po.count(G, P, threads, lo, hi, with_bytes=True)
-            t_pat += time.perf_counter() - t0
+            dt = time.perf_counter() - t0
+            t_pat += dt
             cnt += c
             byts += nb
-            lo, span = hi, span * 2
+            # next prefix: double it, but aim at half the time left at this
+            # chunk's rate (edge costs vary by orders of magnitude)
+            per_edge = dt / max(1, hi - lo)
+            lo, span = hi, max(1, min(span * 2, int(0.5 * (share - t_pat) / max(per_edge, 1e-9))))
         per[name] = (byts, cnt)
         total += cnt
         spent += t_pat
