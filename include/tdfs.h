@@ -49,7 +49,7 @@ typedef struct {
   int edge_stride;      /* level-0 chunks are dealt round-robin over edge_stride */
   int edge_phase;       /*   shards; this call takes chunks == edge_phase (mod) */
   void *stream;         /* cudaStream_t; NULL = legacy default stream */
-  int steal_min;        /* steal / donate only levels with >= steal_min items left (0 auto = 2) */
+  int steal_min;        /* steal only levels with >= steal_min items left (0 auto = 2) */
   int merge_ratio;      /* merge a list whose length <= merge_ratio x the scanned span, else
                            search it (0 auto = 4) */
   int graph_capture;    /* 1: launch through a cached CUDA graph (upload, reset, kernel,
@@ -61,6 +61,9 @@ typedef struct {
                            (0 auto = on, -1 off) */
   int split_after_us;   /* a warp's subtree becomes stealable after this many microseconds
                            on it, donatable to the HBM ring after 4x (0 auto = 150, -1 = at once) */
+  int steal_first;      /* an idle warp first takes a level with >= steal_first items from a warp
+                           of its CTA, then a unit of the split ring, and only then a level
+                           with >= steal_min items (0 auto = 8) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);
@@ -192,7 +195,9 @@ int tdfs_gen_pattern(int k, double density, int nlabels, uint64_t seed, char *bu
  * kernel's exact candidate rules (level-0 edge filter, symmetry conditions or
  * labels, injectivity).  Unbiased for matches and per-depth node counts; the
  * relative standard errors say how far to trust them.  Used to admit or
- * schedule queries by expected work; deterministic for a given seed. */
+ * schedule queries by expected work; deterministic for a given seed.  The
+ * level-0 edge range [edge_begin, edge_end) is as in tdfs_options (0, -1 =
+ * every edge): the estimate of what tdfs_count counts over that range. */
 typedef struct tdfs_estimate_result {
   double matches;                  /* expected count, as tdfs_count reports it */
   double nodes[TDFS_MAX_PATTERN];  /* expected partial matches at each depth 1..k-1 */
@@ -201,7 +206,8 @@ typedef struct tdfs_estimate_result {
   double scanned_rse;              /* relative standard error of `scanned` */
   int64_t probes;
 } tdfs_estimate_result;
-int tdfs_estimate(const tdfs_csr *c, const tdfs_plan *p, int64_t probes, uint64_t seed, tdfs_estimate_result *out);
+int tdfs_estimate(const tdfs_csr *c, const tdfs_plan *p, int64_t edge_begin, int64_t edge_end, int64_t probes,
+                  uint64_t seed, tdfs_estimate_result *out);
 
 #ifdef __cplusplus
 }

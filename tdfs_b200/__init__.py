@@ -66,6 +66,7 @@ class Options(C.Structure):
         ("edge_chunk", C.c_int),
         ("fixed_stage", C.c_int),
         ("split_after_us", C.c_int),
+        ("steal_first", C.c_int),
     ]
 
 
@@ -132,7 +133,7 @@ def lib() -> C.CDLL:
     L.tdfs_gen_chung_lu.argtypes = [i64, i64, C.c_double, i32, C.c_uint64, pp]
     L.tdfs_gen_rmat.argtypes = [ci, ci, C.c_double, C.c_double, C.c_double, C.c_uint64, pp]
     L.tdfs_gen_pattern.argtypes = [ci, C.c_double, ci, C.c_uint64, C.c_char_p, C.c_size_t]
-    L.tdfs_estimate.argtypes = [vp, vp, i64, C.c_uint64, vp]
+    L.tdfs_estimate.argtypes = [vp, vp, i64, i64, i64, C.c_uint64, vp]
     L.tdfs_autotune.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), ci, C.POINTER(Options),
                                 C.POINTER(C.c_float)]
     L.tdfs_count_static.argtypes = [ci, i64, i64, vp, vp, vp, vp, C.POINTER(Options), C.POINTER(C.c_uint64)]
@@ -224,11 +225,13 @@ class EstimateResult(C.Structure):
                 ("matches_rse", C.c_double), ("scanned_rse", C.c_double), ("probes", C.c_int64)]
 
 
-def estimate(csr: HostCSR, pattern: "PatternPreprocessor", probes: int = 1000, seed: int = 0) -> EstimateResult:
-    """Expected count and work of a query (tdfs_estimate), from random DFS probes
-    over the host copy of the graph."""
+def estimate(csr: HostCSR, pattern: "PatternPreprocessor", probes: int = 1000, seed: int = 0,
+             edge_begin: int = 0, edge_end: int = -1) -> EstimateResult:
+    """Expected count and work of a query (tdfs_estimate) over the level-0 edge
+    range [edge_begin, edge_end), from random DFS probes over the host copy
+    of the graph."""
     r = EstimateResult()
-    _check(lib().tdfs_estimate(csr._h, pattern._h, probes, seed, C.byref(r)))
+    _check(lib().tdfs_estimate(csr._h, pattern._h, edge_begin, edge_end, probes, seed, C.byref(r)))
     return r
 
 

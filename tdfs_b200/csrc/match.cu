@@ -701,9 +701,9 @@ struct Engine {
   // the victim's word (gen | next | end) down to the split point.  The copy is
   // valid iff the CAS succeeds: a warp rewrites its items, prefix, plan or
   // slot only after bumping gen.  Returns the level (1 = edge pairs) or 0.
-  __device__ int steal_local(int nwarps, int me) {
+  __device__ int steal_local(int nwarps, int me, int min_items) {
     // one pass: lane v scans warp v's levels and offers its shallowest level
-    // with at least steal_min items; the warp takes the shallowest offer,
+    // with at least min_items items; the warp takes the shallowest offer,
     // the largest one on ties
     unsigned long long key = 0;
     const unsigned long long now = now_ns();
@@ -713,7 +713,7 @@ struct Engine {
       for (int l = 1; l <= kMaxK - 2; ++l) {
         const unsigned long long w = *(volatile const unsigned long long *)&V.word[l];
         const int rem = (int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu);
-        if (rem >= cfg.steal_min) {
+        if (rem >= min_items) {
           key = ((unsigned long long)(kMaxK - l) << 40) | ((unsigned long long)rem << 8) | (unsigned)lane;
           break;
         }
@@ -733,7 +733,7 @@ struct Engine {
     w = __shfl_sync(kFull, w, 0);
     __threadfence_block();
     const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
-    if (n - it < cfg.steal_min) return 0;
+    if (n - it < min_items) return 0;
     const int vslot = *(volatile int32_t *)&V.slot;
     if (vslot < 0) return 0;
     const int take = (n - it) / 2;
@@ -941,7 +941,9 @@ struct Engine {
         level = 0;
         if (take_tickets()) level = base = 1;
         if (!level && cfg.steal) {
-          int l = steal_local(nwarps, me);
+          // largest grains first: a big share of a CTA neighbour's level, a
+          // split unit from the ring (work of other SMs), then any remainder
+          int l = steal_local(nwarps, me, max(cfg.steal_first, cfg.steal_min));
           if (!l) {
             int nonempty = 0;
             if (lane == 0) {
@@ -951,6 +953,7 @@ struct Engine {
             }
             if (__shfl_sync(kFull, nonempty, 0)) l = queue_pop();
           }
+          if (!l && cfg.steal_min < cfg.steal_first) l = steal_local(nwarps, me, cfg.steal_min);
           if (l) level = base = l;
         }
         if (level) {

@@ -56,6 +56,8 @@ struct KernelCfg {
   int32_t split_after_ns;  // work becomes stealable after this long on one base subtree
                            // (donation to the HBM ring after 4x as long)
   int32_t wide_regs;    // 1: the 80-register build (at most 3 CTAs of 256 threads per SM)
+  int32_t steal_first;  // first look for levels with >= steal_first items, then the ring, then steal_min
+  int32_t pad_;
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
