@@ -105,21 +105,33 @@ inline size_t draw(const tdfs_csr &g, const int32_t *xs, size_t n, int a, Rng &r
 // size.  The path weight is the product of 1 / probability, which keeps
 // every per-depth estimate unbiased (importance sampling of Knuth's
 // estimator).
-void probe(const tdfs_csr &g, const Tables &tab, const DevPlan &P, const int *pw, Rng &rng, Acc &a,
-           std::vector<int32_t> &cand) {
+void probe(const tdfs_csr &g, const Tables &tab, const DevPlan &P, const int *pw, int64_t eb, int64_t ee,
+           Rng &rng, Acc &a, std::vector<int32_t> &cand) {
   const bool lab = P.labeled != 0;
   double probe_matches = 0, probe_scanned = 0;
-  // level 0: source r ~ deg^max(pw0, 1) (pw0 = 1 is a uniform directed edge),
-  // then c ~ deg^pw1 among r's neighbours
-  const int a0 = std::max(pw[0], 1);
-  const std::vector<double> &cum = tab.cum[a0];
-  const double u = rng.uniform() * cum.back();
-  const int32_t r = (int32_t)(std::upper_bound(cum.begin(), cum.end(), u) - cum.begin() - 1);
-  const int32_t dr = degree(g, r);
-  if (r < 0 || r >= g.n || dr == 0) return;  // u landed on a zero-weight edge of the table
-  double pr = dpow(dr, a0) / cum.back(), pc;
-  const int32_t *nr = g.colidx.data() + g.rowptr[r];
-  const int32_t c = nr[draw(g, nr, (size_t)dr, pw[1], rng, &pc)];
+  int32_t r, c, dr;
+  double pr, pc;
+  if (eb == 0 && ee == g.nedges) {
+    // whole graph: source r ~ deg^max(pw0, 1) (pw0 = 1 is a uniform directed
+    // edge), then c ~ deg^pw1 among r's neighbours
+    const int a0 = std::max(pw[0], 1);
+    const std::vector<double> &cum = tab.cum[a0];
+    const double u = rng.uniform() * cum.back();
+    r = (int32_t)(std::upper_bound(cum.begin(), cum.end(), u) - cum.begin() - 1);
+    if (r < 0 || r >= g.n || degree(g, r) == 0) return;  // u landed on a zero-weight end of the table
+    dr = degree(g, r);
+    pr = dpow(dr, a0) / cum.back();
+    const int32_t *nr = g.colidx.data() + g.rowptr[r];
+    c = nr[draw(g, nr, (size_t)dr, pw[1], rng, &pc)];
+  } else {
+    // a level-0 edge range (a shard or a bench slice): a uniform edge of it
+    const int64_t e = eb + (int64_t)rng.below((uint64_t)(ee - eb));
+    r = (int32_t)(std::upper_bound(g.rowptr.begin(), g.rowptr.end(), e) - g.rowptr.begin() - 1);
+    c = g.colidx[e];
+    dr = degree(g, r);
+    pr = 1.0 / (double)(ee - eb);
+    pc = 1.0;
+  }
   bool ok = true;
   if (!lab && P.orient && !(r < c)) ok = false;
   if (ok && lab && (g.labels[r] != P.label[0] || g.labels[c] != P.label[1])) ok = false;
@@ -192,15 +204,17 @@ void probe(const tdfs_csr &g, const Tables &tab, const DevPlan &P, const int *pw
 
 using namespace tdfs;
 
-extern "C" int tdfs_estimate(const tdfs_csr *g, const tdfs_plan *p, int64_t probes, uint64_t seed,
-                             tdfs_estimate_result *out) {
+extern "C" int tdfs_estimate(const tdfs_csr *g, const tdfs_plan *p, int64_t edge_begin, int64_t edge_end,
+                             int64_t probes, uint64_t seed, tdfs_estimate_result *out) {
   if (!g || !p || !out) return fail(TDFS_ERR_ARG, "null argument");
   if (probes < 1) return fail(TDFS_ERR_ARG, "probes must be >= 1");
+  const int64_t eb = std::max<int64_t>(0, edge_begin);
+  const int64_t ee = (edge_end < 0 || edge_end > g->nedges) ? g->nedges : edge_end;
   const DevPlan &P = plan_device_table(p);
   if (P.labeled && g->labels.empty()) return fail(TDFS_ERR_ARG, "labeled pattern on a graph without labels");
   std::memset(out, 0, sizeof *out);
   out->probes = probes;
-  if (g->nedges == 0) return TDFS_OK;
+  if (ee <= eb) return TDFS_OK;
   // proposal exponents: forward neighbours of each pattern vertex, capped
   int pw[kMaxK] = {};
   for (int j = 1; j < P.k; ++j)
@@ -215,7 +229,7 @@ extern "C" int tdfs_estimate(const tdfs_csr *g, const tdfs_plan *p, int64_t prob
       const int64_t lo = probes * b / kBlocks, hi = probes * (b + 1) / kBlocks;
       for (int64_t j = lo; j < hi; ++j) {
         Rng rng(hash64(seed, (uint64_t)j));
-        probe(*g, tab, P, pw, rng, block[b], cand);
+        probe(*g, tab, P, pw, eb, ee, rng, block[b], cand);
       }
     }
   };

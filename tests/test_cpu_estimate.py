@@ -86,3 +86,22 @@ def test_deterministic_per_seed_and_errors(T, er_pair):
     with pytest.raises(T.TdfsError) as e:
         T.estimate(unl, T.PatternPreprocessor(text=TRIANGLE, labeled=True), 10, 1)
     assert e.value.code == ARG
+
+
+def test_edge_range_estimates_sum_to_whole(T, po):
+    """Estimates over level-0 edge ranges are unbiased for the counts over
+    those ranges (the oracle counts the same ranges)."""
+    g = T.gen_chung_lu(20000, 60000, 2.1, 600, 1)
+    O = po.Graph(g.rowptr.copy(), g.colidx.copy(), None)
+    P = T.PatternPreprocessor(text=CYCLE4)
+    E = g.nedges
+    nonzero = 0
+    for b, e in ((0, E // 10), (E // 3, E // 3 + 5000), (E // 2, E // 2 + 20000), (E - 4000, E)):
+        want = po.count(O, po.Plan(CYCLE4, False), edge_begin=b, edge_end=e)
+        r = T.estimate(g, P, 20000, 7, edge_begin=b, edge_end=e)
+        if want == 0:
+            assert r.matches == 0
+        elif want >= 100:  # (a handful of matches in a large tree is missed by every probe)
+            assert abs(r.matches - want) <= 5 * r.matches_rse * r.matches, (b, e, r.matches, want)
+            nonzero += 1
+    assert nonzero >= 2
