@@ -130,6 +130,15 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
         self.proc.wait(timeout=10)
+        after = False
+        if not self.rows:  # a timed region shorter than the 200 ms period: one reading right after it
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=30)
+                self.rows = [[x.strip() for x in l.split(",")] for l in out.stdout.splitlines() if l.strip()]
+                after = True
+            except (OSError, subprocess.SubprocessError):
+                pass
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in self.rows:
@@ -141,8 +150,21 @@ class ClockSampler:
                         reasons.add(n)
             except (ValueError, IndexError):
                 pass
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        rec = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+               "samples": 0 if after else len(sm)}
+        if after:
+            rec["sampled"] = "once, right after the timed region (shorter than the sampling period)"
+        return rec
+
+
+def measured_traffic(workload):
+    """DRAM bytes per timed match-kernel launch of this workload from the ncu
+    capture summarised in profiles/match_kernel_traffic.json, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "match_kernel_traffic.json")) as f:
+            return json.load(f)[workload]["dram_bytes_per_launch"]
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def measured_hbm_peak():
@@ -498,7 +520,10 @@ def main():
             mean_s = statistics.mean(ms for _, ms, _ in usable) / 1e3
             achieved = mean_b / mean_s / 1e9
             line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                                "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                                "frac": achieved / peak, "peak_kind": kind,
+                                "traffic": measured_traffic(args.workload),
+                                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per timed "
+                                                  "launch, profiles/match_kernel_traffic.json",
                                 "bytes_per_launch": mean_b, "mean_launch_ms": mean_s * 1e3,
                                 "bytes_model": "reference-plan merge model (4 B x (|set1|+|set2|) per set op, "
                                                "16 B per list lookup, 8 B per level-0 edge); bytes per match "
