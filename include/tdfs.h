@@ -54,7 +54,7 @@ typedef struct {
                            search it (0 auto = 4) */
   int graph_capture;    /* 1: launch through a cached CUDA graph (upload, reset, kernel,
                            read-back captured once per launch shape and batch size) */
-  int edge_chunk;       /* directed edges per level-0 ticket: 8, 16, 32 (0 auto; 32 whenever
+  int edge_chunk;       /* directed edges per level-0 ticket: 1, 2, 4, ..., 32 (0 auto; 32 whenever
                            edge_stride > 1, the chunk the round-robin dealing is defined on) */
   int fixed_stage;      /* last vertex: stage the intersection of its backward neighbours
                            other than the parent once per parent in shared memory

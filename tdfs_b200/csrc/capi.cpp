@@ -89,8 +89,8 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
   if (c.steal_first < 2 || c.steal_first > 4096) return fail(TDFS_ERR_ARG, "steal_first must lie in [2, 4096]");
-  if (o.edge_chunk != 0 && o.edge_chunk != 8 && o.edge_chunk != 16 && o.edge_chunk != 32)
-    return fail(TDFS_ERR_ARG, "edge_chunk must be 0, 8, 16 or 32");
+  if (o.edge_chunk < 0 || o.edge_chunk > 32 || (o.edge_chunk & (o.edge_chunk - 1)) != 0)
+    return fail(TDFS_ERR_ARG, "edge_chunk must be 0 or a power of two up to 32");
   const size_t smem = (size_t)c.warp_bytes * s.warps_per_block;
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
@@ -495,7 +495,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::steal_min, {2, 8, 32}},
       {&tdfs_options::steal_first, {2, 8, 32}},
       {&tdfs_options::blocks_per_sm, {1, 2, 3}},
-      {&tdfs_options::edge_chunk, {8, 16, 32}},
+      {&tdfs_options::edge_chunk, {1, 4, 8, 32}},
       {&tdfs_options::fixed_stage, {-1, 1}},
       {&tdfs_options::split_after_us, {-1, 5, 50, 150, 500}},
   };

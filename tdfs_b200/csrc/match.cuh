@@ -62,14 +62,17 @@ struct KernelCfg {
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
 
-// Edges per level-0 ticket: 32 when the range is dealt over several shards
-// (the documented round-robin split), else the largest of 32/16/8 that still
-// gives every warp of the grid about two tickets to start with.
+// Edges per level-0 ticket: a requested power of two up to 32; else 32 when
+// the range is dealt over several shards (the documented round-robin split),
+// else the largest power of two that still gives every warp of the grid two
+// tickets to start with -- down to single edges for the short ranges of a
+// power-law slice, whose heavy edges then start on different warps instead
+// of waiting in one warp's ticket to be stolen.
 inline int auto_chunk(int64_t edges, int stride, int total_warps, int requested) {
-  if (requested == 8 || requested == 16 || requested == 32) return requested;
+  if (requested > 0 && requested <= kEdgeChunk && (requested & (requested - 1)) == 0) return requested;
   if (stride > 1) return kEdgeChunk;
   int c = kEdgeChunk;
-  while (c > 8 && edges / c < 2ll * total_warps) c >>= 1;
+  while (c > 1 && edges / c < 2ll * total_warps) c >>= 1;
   return c;
 }
 

@@ -28,6 +28,8 @@ OPTION_SETS = [
     {"chunk_cap": 64, "warps_per_block": 4},         # tiny buffers: many refills
     {"merge_window": 256, "chunk_cap": 128, "blocks_per_sm": 1},
     {"fixed_stage": -1, "edge_chunk": 32, "steal_min": 8},  # no last-level staging
+    {"edge_chunk": 1, "steal_first": 2, "split_after_us": -1},  # one edge per ticket, eager splits
+    {"edge_chunk": 4, "blocks_per_sm": 2, "steal_first": 32},
 ]
 
 
