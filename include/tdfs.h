@@ -64,6 +64,9 @@ typedef struct {
   int steal_first;      /* an idle warp first takes a level with >= steal_first items from a warp
                            of its CTA, then a unit of the split ring, and only then a level
                            with >= steal_min items (0 auto = 8) */
+  int lane_list;        /* last level with a staged fixed set: a parent whose adjacency list is
+                           at most this long is counted by one lane, 32 parents at once
+                           (0 auto = 8, -1 off: one parent per warp pass) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

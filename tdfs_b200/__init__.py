@@ -67,6 +67,7 @@ class Options(C.Structure):
         ("fixed_stage", C.c_int),
         ("split_after_us", C.c_int),
         ("steal_first", C.c_int),
+        ("lane_list", C.c_int),
     ]
 
 

@@ -86,9 +86,11 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.idle_ms = 30000;
   c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
   c.steal_first = o.steal_first > 0 ? o.steal_first : 8;
+  c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 8);
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
   if (c.steal_first < 2 || c.steal_first > 4096) return fail(TDFS_ERR_ARG, "steal_first must lie in [2, 4096]");
+  if (c.lane_list > 4096) return fail(TDFS_ERR_ARG, "lane_list must be at most 4096");
   if (o.edge_chunk < 0 || o.edge_chunk > 32 || (o.edge_chunk & (o.edge_chunk - 1)) != 0)
     return fail(TDFS_ERR_ARG, "edge_chunk must be 0 or a power of two up to 32");
   const size_t smem = (size_t)c.warp_bytes * s.warps_per_block;
@@ -494,6 +496,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::steal, {0, 1}},
       {&tdfs_options::steal_min, {2, 8, 32}},
       {&tdfs_options::steal_first, {2, 8, 32}},
+      {&tdfs_options::lane_list, {-1, 16, 64}},
       {&tdfs_options::blocks_per_sm, {1, 2, 3}},
       {&tdfs_options::edge_chunk, {1, 4, 8, 32}},
       {&tdfs_options::fixed_stage, {-1, 1}},

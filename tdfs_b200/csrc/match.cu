@@ -401,11 +401,8 @@ struct Engine {
   }
 
   __device__ unsigned long long count_fixed(int i) {
-    const int par = i - 1;
-    const int32_t x = W.phi[par];
-    const int32_t *F = fbuf();
-    const int32_t nF = W.fn;
-    if (nF == 0) return 0;
+    const int32_t x = W.phi[i - 1];
+    if (W.fn == 0) return 0;
     int64_t b = 0, e = 0;
     if (lane == 0) {
       b = G.rowptr[x];
@@ -413,10 +410,63 @@ struct Engine {
     }
     b = __shfl_sync(kFull, b, 0);
     e = __shfl_sync(kFull, e, 0);
+    return count_fixed_list(i, x, b, e);
+  }
+
+  // The condition between the last vertex i and its parent: 1 = y > x,
+  // 2 = y < x, 0 = y != x.
+  __device__ __forceinline__ int parent_rel(int i) const {
+    return LAB ? 0 : (P.larger[i] >> (i - 1) & 1) ? 1 : (P.less[i] >> (i - 1) & 1) ? 2 : 0;
+  }
+
+  // Last level over a batch of b parents (items[0..b), b <= 32) that share
+  // the fixed set F: lane j counts |F ∩ N(items[j])| by itself when that list
+  // is at most cfg.lane_list long -- 32 short lists at once, their memory
+  // latencies overlapped, instead of one warp-wide pass per parent with most
+  // lanes idle -- and the longer lists are counted by the whole warp after.
+  __device__ unsigned long long count_fixed_batch(int i, const int32_t *items, int b) {
+    const int32_t *F = fbuf();
+    const int32_t nF = W.fn;
+    if (nF == 0) return 0;
+    const int rel = parent_rel(i);
+    const bool mine = lane < b;
+    const int32_t x = mine ? items[lane] : 0;
+    int64_t rb = 0, re = 0;
+    if (mine) {
+      rb = G.rowptr[x];
+      re = G.rowptr[x + 1];
+    }
+    const bool alone = mine && re - rb <= (int64_t)cfg.lane_list;
+    unsigned c = 0;
+    if (alone) {
+      const int32_t *L = G.colidx + rb;
+      const int32_t len = (int32_t)(re - rb);
+      int32_t q = 0;  // F cursor: L is sorted, so each search starts where the last ended
+      for (int32_t t = 0; t < len && q < nF; ++t) {
+        const int32_t y = L[t];
+        if (rel == 1 ? y <= x : rel == 2 ? y >= x : y == x) continue;
+        q = lower_bound(F, q, nF, y);
+        c += q < nF && F[q] == y;
+      }
+    }
+    unsigned long long total = __reduce_add_sync(kFull, c);
+    unsigned rest = __ballot_sync(kFull, mine && !alone);
+    while (rest) {
+      const int j = __ffs(rest) - 1;
+      rest &= rest - 1;
+      total += count_fixed_list(i, __shfl_sync(kFull, x, j), __shfl_sync(kFull, rb, j), __shfl_sync(kFull, re, j));
+    }
+    return total;
+  }
+
+  // |F ∩ N(x)| under the parent condition, the warp together; N(x) is
+  // colidx[b, e).
+  __device__ unsigned long long count_fixed_list(int i, int32_t x, int64_t b, int64_t e) {
+    const int32_t *F = fbuf();
+    const int32_t nF = W.fn;
     const int32_t *L = G.colidx + b;
     const int32_t len = (int32_t)(e - b);
-    // the condition between the last vertex y and its parent x
-    const int rel = LAB ? 0 : (P.larger[i] >> par & 1) ? 1 : (P.less[i] >> par & 1) ? 2 : 0;
+    const int rel = parent_rel(i);
     unsigned long long c = 0;
     if ((int64_t)len <= 4ll * nF) {
       // scan N(x) (coalesced), look each y up in F (shared memory)
@@ -505,6 +555,36 @@ struct Engine {
       c += __popc(__ballot_sync(kFull, ok));
     }
     return c;
+  }
+
+  // Claim up to 32 consecutive buffered candidates of stored level l (one
+  // CAS): all of them while no warp is hungry, else at most half of what is
+  // left, so that the other half stays stealable.  Returns the first index
+  // and sets *b to how many (0 when none).
+  __device__ int32_t claim_batch(int l, int *b) {
+    int32_t r = -1, got = 0;
+    if (lane == 0) {
+      const bool share = cfg.steal && *(volatile int32_t *)&ctl->hungry > 0;
+      unsigned long long w = *(volatile unsigned long long *)&W.word[l];
+      for (int tries = 0;; ++tries) {
+        const uint32_t it = (uint32_t)(w >> 16) & 0xffffu, n = (uint32_t)w & 0xffffu;
+        if (it >= n) break;
+        if (tries >= kCasLimit) {
+          raise_error(ctl, TDFS_ERR_TIMEOUT);
+          break;
+        }
+        const uint32_t take = min(32u, share ? max(1u, (n - it) / 2) : n - it);
+        const unsigned long long old = atomicCAS(&W.word[l], w, w + ((unsigned long long)take << 16));
+        if (old == w) {
+          r = (int32_t)it;
+          got = (int)take;
+          break;
+        }
+        w = old;
+      }
+    }
+    *b = __shfl_sync(kFull, got, 0);
+    return __shfl_sync(kFull, r, 0);
   }
 
   // Claim the next buffered candidate of stored level l; -1 when none.
@@ -982,6 +1062,19 @@ struct Engine {
         if (done) break;
         if (!wait_for_work()) break;
         continue;
+      }
+      if (cfg.lane_list > 0 && level >= 2 && level + 1 == P.k - 1 && fixed_applies(level + 1)) {
+        // last stored level: batches of items, short lists counted one per lane
+        if (W.fvalid == 0) build_fixed(level + 1);
+        if (W.fvalid == 1) {
+          int b = 0;
+          const int32_t first = claim_batch(level, &b);
+          if (b > 0) {
+            count += count_fixed_batch(level + 1, buf(level) + first, b);
+            if (cfg.steal) maybe_donate(level);
+            continue;
+          }
+        }
       }
       const int32_t idx = claim(level);
       if (idx >= 0) {
