@@ -4,7 +4,8 @@
     python bench.py [--gpus N --steps K --warmup W] [--workload c2] [--impl tdfs|reference]
 
 One step = every pattern of the workload counted over one batch of level-0
-edges, the graph already resident in HBM: the whole edge array for the small
+edges in one batched launch (tdfs_count_batch), the graph already resident in
+HBM: the whole edge array for the small
 configs (c1, c3), one contiguous 1/1000 slice of it for the power-law config
 (c2; its house count is ~1e13 matches, about 25 GPU-minutes for the whole
 graph) and a 1/500000 slice for the scale-24 R-MAT graph (c4; its 6-clique
@@ -228,7 +229,8 @@ def run_tdfs(args, rank, world, dist):
         return T.shard_options(rank, world, edge_begin=rng[0], edge_end=rng[1])
 
     def step(graph, rng):
-        return [T.count(graph, p, opts(rng)) for _, p in plans]
+        # every pattern of the step in one persistent launch (tdfs_count_batch)
+        return T.count_batch(graph, [p for _, p in plans], opts(rng))
 
     for r in warm_r:
         step(G, r)
@@ -238,17 +240,17 @@ def run_tdfs(args, rank, world, dist):
     clocks = ClockSampler(dev)
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in timed_r]
-    launch = []        # (pattern, kernel ms, count) per match-kernel launch
+    launch = []        # ({pattern: count}, kernel ms) per match-kernel launch
     per_pattern = {n: 0 for n, _ in plans}
     torch.cuda.synchronize()
     for s, r in enumerate(timed_r):
         flush.zero_()  # L2 flush between timed steps (256 MB > 126 MB L2), outside the events
         ev[s][0].record()
-        res = step(G, r)
+        counts, kms = step(G, r)
         ev[s][1].record()
-        for (n, _), x in zip(plans, res):
-            launch.append((n, x.kernel_ms, x.count))
-            per_pattern[n] += x.count
+        launch.append(({n: c for (n, _), c in zip(plans, counts)}, kms))
+        for (n, _), c in zip(plans, counts):
+            per_pattern[n] += c
     torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     if dist:
@@ -278,7 +280,7 @@ def run_tdfs(args, rank, world, dist):
         Gh = T.GraphPreprocessor(rowptr=rp.numpy(), colidx=ci.numpy(), labels=None if lb is None else lb.numpy(),
                                  labeled=labeled, device=dev)
         ps = [T.PatternPreprocessor(text=t, labeled=labeled) for _, t in pats]
-        e2e_m += sum(T.count(Gh, p, opts(r)).count for p in ps)
+        e2e_m += sum(T.count_batch(Gh, ps, opts(r))[0])
         Gh.close()
         e2e_s += time.perf_counter() - t0
     if dist:
@@ -299,7 +301,7 @@ def run_tdfs(args, rank, world, dist):
                        counts=per_pattern),
         "e2e": {"value": e2e_m / e2e_s, "unit": "matches/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": 2 * len(pats) * args.steps,
+        "gpu_launches": 2 * args.steps,  # per step: the control reset and one batched match kernel
         "clocks": clk,
     }
     return line, launch, (g, pats, labeled, timed_r)
@@ -325,12 +327,14 @@ def run_reference(args, rank, world):
     prefix = os.path.join(work, "snap.txt")
     g.write(prefix)
 
-    def run(text, ranges):
+    def run(text, warm, ranges):
+        # warm-up launches first, in the same process, untimed (-w)
         p = os.path.join(work, "p.g")
         with open(p, "w") as f:
             f.write(text)
-        args_r = [str(x) for r in ranges for x in r]
-        r = subprocess.run([exe, prefix, p] + args_r, capture_output=True, text=True, timeout=args.ref_timeout)
+        args_r = [str(x) for r in warm + ranges for x in r]
+        r = subprocess.run([exe, prefix, p, "-w", str(len(warm))] + args_r, capture_output=True, text=True,
+                           timeout=args.ref_timeout)
         lines = [l for l in r.stdout.splitlines() if l.count("\t") == 2]
         if r.returncode or not lines:
             raise RuntimeError(f"reference run failed rc={r.returncode}: {r.stderr[-300:]}")
@@ -338,11 +342,9 @@ def run_reference(args, rank, world):
         return float(ms), int(c)
 
     try:
-        for _, t in pats:
-            run(t, warm_r)
         tot_ms, tot_c, counts = 0.0, 0, {}
         for n, t in pats:
-            ms, c = run(t, timed_r)
+            ms, c = run(t, warm_r, timed_r)
             tot_ms += ms
             tot_c += c
             counts[n] = c
@@ -356,7 +358,8 @@ def run_reference(args, rank, world):
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32/u64",
             "data": "synthetic (seeded generators of the benchmark config)",
             "config": dict(desc, counts=counts, timed_edge_ranges=timed_r,
-                           timing="the reference's own kernel, cudaEvent pair around each launch as cu_test.cu:81-97",
+                           timing="the reference's own kernel, cudaEvent pair around each launch as cu_test.cu:81-97; "
+                                  "the warm-up launches run first in the same process, untimed",
                            note="the reference build's counts can differ from the reference semantics on heavy "
                                 "subtrees; they are reported as printed"),
             "cpu_baseline": {"value": value, "unit": "matches/s", "cores": 0, "kind": "reference",
@@ -512,12 +515,14 @@ def main():
         else:
             line["cpu_baseline"] = None
         # roofline of the match kernel: merge-model bytes per match (oracle
-        # sample, per pattern) x matches per launch / mean launch time
-        usable = [(n, ms, c) for n, ms, c in launch if n in per and per[n][1] > 0 and ms > 0]
-        if usable:
-            bytes_launch = [per[n][0] / per[n][1] * c for n, ms, c in usable]
+        # sample, per pattern) x each pattern's matches in the launch / mean
+        # launch time
+        usable = [(cs, ms) for cs, ms in launch if ms > 0]
+        if usable and any(n in per and per[n][1] > 0 for n in usable[0][0]):
+            bytes_launch = [sum(per[n][0] / per[n][1] * c for n, c in cs.items() if n in per and per[n][1] > 0)
+                            for cs, _ in usable]
             mean_b = statistics.mean(bytes_launch)
-            mean_s = statistics.mean(ms for _, ms, _ in usable) / 1e3
+            mean_s = statistics.mean(ms for _, ms in usable) / 1e3
             achieved = mean_b / mean_s / 1e9
             line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                 "frac": achieved / peak, "peak_kind": kind,

@@ -3,7 +3,11 @@
 // level-0 edge ranges, so the reference can be timed on the same bounded
 // slices of a workload as this repository's engine.
 //
-//   refshard_{ulb,lb} <graph prefix> <pattern.g> <begin> <end> [<begin> <end> ...]
+//   refshard_{ulb,lb} <graph prefix> <pattern.g> [-w K] <begin> <end> [<begin> <end> ...]
+//
+// With -w K the first K ranges are warm-up launches in the same process
+// (module loading and first-touch costs land there) and are neither timed
+// nor counted.
 //
 // Set-up follows the reference driver (cu_test.cu:14-78): the reference's
 // GraphPreprocessor / PatternPreprocessor / build_src_vtx / to_gpu, per-warp
@@ -38,8 +42,13 @@ using namespace STMatch;
 static const int kQueueCapTriples = 1000000;  // TIMEOUT_QUEUE_CAP, cu_test.cu:8
 
 int main(int argc, char **argv) {
-  if (argc < 5 || (argc - 3) % 2) {
-    fprintf(stderr, "usage: %s <prefix> <pattern.g> <begin> <end> [<begin> <end> ...]\n", argv[0]);
+  int first = 3, warm = 0;
+  if (argc > 4 && std::strcmp(argv[3], "-w") == 0) {
+    warm = std::atoi(argv[4]);
+    first = 5;
+  }
+  if (argc < first + 2 || (argc - first) % 2 || warm < 0) {
+    fprintf(stderr, "usage: %s <prefix> <pattern.g> [-w K] <begin> <end> [<begin> <end> ...]\n", argv[0]);
     return 2;
   }
   CK(cudaSetDevice(0));
@@ -90,7 +99,7 @@ int main(int argc, char **argv) {
   CK(cudaEventCreate(&stop));
   unsigned long long total = 0;
   double total_ms = 0;
-  for (int a = 3; a + 1 < argc; a += 2) {
+  for (int a = first, r = 0; a + 1 < argc; a += 2, ++r) {
     const long begin = std::atol(argv[a]), end = std::atol(argv[a + 1]);
     if (begin < 0 || end < begin || end > g.g.nedges) {
       fprintf(stderr, "bad range %ld %ld\n", begin, end);
@@ -110,8 +119,9 @@ int main(int argc, char **argv) {
     CK(cudaGetLastError());
     float ms = 0;
     CK(cudaEventElapsedTime(&ms, start, stop));
-    total_ms += ms;
     CK(cudaMemcpy(res.data(), gpu_res, sizeof(size_t) * NWARPS_TOTAL, cudaMemcpyDeviceToHost));
+    if (r < warm) continue;  // warm-up launch
+    total_ms += ms;
     for (int i = 0; i < NWARPS_TOTAL; i++) total += res[i];
   }
   if (!LABELED) total *= p.PatternMultiplicity;
