@@ -493,7 +493,8 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::chunk_cap, {128, 256, 512, 1024}},
       {&tdfs_options::merge_window, {-1, 128, 256}},
       {&tdfs_options::merge_ratio, {1, 4, 16}},
-      {&tdfs_options::steal, {0, 1}},
+      // (stealing stays on: without it one warp keeps a hub's whole subtree,
+      // minutes on a power-law slice, and a launch cannot be cut short)
       {&tdfs_options::steal_min, {2, 8, 32}},
       {&tdfs_options::steal_first, {2, 8, 32}},
       {&tdfs_options::lane_list, {-1, 16, 64}},
