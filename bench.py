@@ -158,6 +158,17 @@ class ClockSampler:
         return rec
 
 
+def reduce_over_ranks(dist, seconds_or_ms, counts, device="cuda"):
+    """Whole-job figures over the ranks: the slowest rank's time (max) and the
+    summed counts.  `counts` is a list of ints; returns (time, counts)."""
+    import torch
+    t = torch.tensor([seconds_or_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    m = torch.tensor(list(counts), dtype=torch.int64, device=device)
+    dist.all_reduce(m)
+    return float(t.item()), [int(v) for v in m.tolist()]
+
+
 def measured_traffic(workload):
     """DRAM bytes per timed match-kernel launch of this workload from the ncu
     capture summarised in profiles/match_kernel_traffic.json, or None."""
@@ -258,12 +269,8 @@ def run_tdfs(args, rank, world, dist):
     clk = clocks.stop()
     total_ms = sum(step_ms)
     if dist:
-        t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        m = torch.tensor(list(per_pattern.values()), dtype=torch.int64, device="cuda")
-        dist.all_reduce(m)
-        per_pattern = {n: int(v) for n, v in zip(per_pattern, m.tolist())}
+        total_ms, summed = reduce_over_ranks(dist, total_ms, per_pattern.values())
+        per_pattern = dict(zip(per_pattern, summed))
     matches = sum(per_pattern.values())
     value = matches / (total_ms / 1e3)
 
@@ -284,12 +291,7 @@ def run_tdfs(args, rank, world, dist):
         Gh.close()
         e2e_s += time.perf_counter() - t0
     if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-        m = torch.tensor([e2e_m], dtype=torch.int64, device="cuda")
-        dist.all_reduce(m)
-        e2e_m = int(m.item())
+        e2e_s, (e2e_m,) = reduce_over_ranks(dist, e2e_s, [e2e_m])
 
     line = {
         "metric": "matches_per_s", "value": value, "unit": "matches/s", "n_gpus": world,

@@ -64,3 +64,34 @@ def test_shard_ranges_partition_edges():
         for r in range(world):
             seen += [e for b, en in T.shard_edge_ranges(n, r, world) for e in range(b, en)]
         assert sorted(seen) == list(range(n))
+
+
+def _bench_rank_main(rank, world, port, q):
+    import sys
+    sys.path.insert(0, os.path.abspath(os.path.join(os.path.dirname(__file__), "..")))
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    # rank r timed 100 + r ms and counted r + 1, 10 * (r + 1) for two patterns
+    t, counts = bench.reduce_over_ranks(dist, 100.0 + rank, [rank + 1, 10 * (rank + 1)], device="cpu")
+    q.put((rank, t, counts))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_bench_reduces_max_time_and_summed_counts():
+    """The N-rank bench line: the slowest rank's time, every rank's counts."""
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bench_rank_main, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for _, t, counts in got:  # every rank ends with the same whole-job figures
+        assert t == 101.0 and counts == [3, 30]
