@@ -158,6 +158,21 @@ class ClockSampler:
         return rec
 
 
+def deal_chunk(edges, world):
+    """Level-0 chunk for dealing one step's edges over `world` ranks (0: the
+    library's own choice on one rank).  Every rank computes it from the same
+    inputs, so all deal the same chunks: the largest power of two up to 32
+    that still gives each rank about two tickets per warp of a 3552-warp grid
+    (148 SMs x 3 CTAs x 8 warps) -- single edges on a short power-law slice,
+    whose heavy edges then spread over the ranks."""
+    if world == 1:
+        return 0
+    c = 32
+    while c > 1 and edges // c < 2 * 3552 * world:
+        c //= 2
+    return c
+
+
 def reduce_over_ranks(dist, seconds_or_ms, counts, device="cuda"):
     """Whole-job figures over the ranks: the slowest rank's time (max) and the
     summed counts.  `counts` is a list of ints; returns (time, counts)."""
@@ -237,7 +252,8 @@ def run_tdfs(args, rank, world, dist):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def opts(rng):
-        return T.shard_options(rank, world, edge_begin=rng[0], edge_end=rng[1])
+        return T.shard_options(rank, world, edge_begin=rng[0], edge_end=rng[1],
+                               edge_chunk=deal_chunk(rng[1] - rng[0], world))
 
     def step(graph, rng):
         # every pattern of the step in one persistent launch (tdfs_count_batch)

@@ -343,21 +343,25 @@ EDGE_CHUNK = 32  # directed edges per level-0 ticket (kEdgeChunk in match.cuh)
 def shard_options(rank: int, world: int, **kw) -> Options:
     """Options for rank `rank` of `world` GPUs: level-0 edge chunks are dealt
     round-robin, chunk t going to rank t % world, so the ranks' counts sum to
-    the whole count with no data-path collective (one u64 reduction)."""
+    the whole count with no data-path collective (one u64 reduction).  The
+    chunk is 32 edges unless edge_chunk is given; every rank must use the
+    same chunk."""
     if not 0 <= rank < world:
         raise ValueError("rank out of range")
     return default_options(edge_stride=world, edge_phase=rank, **kw)
 
 
-def shard_edge_ranges(nedges: int, rank: int, world: int):
-    """The [begin, end) edge ranges rank `rank` covers under shard_options."""
+def shard_edge_ranges(nedges: int, rank: int, world: int, chunk: int = EDGE_CHUNK, begin: int = 0):
+    """The [begin, end) edge ranges rank `rank` covers under shard_options
+    over the level-0 range [begin, nedges) with `chunk`-edge chunks (the
+    kernel's ticket t covers begin + (t * world + rank) * chunk)."""
     out = []
     t = 0
     while True:
-        b = (t * world + rank) * EDGE_CHUNK
+        b = begin + (t * world + rank) * chunk
         if b >= nedges:
             return out
-        out.append((b, min(nedges, b + EDGE_CHUNK)))
+        out.append((b, min(nedges, b + chunk)))
         t += 1
 
 

@@ -95,3 +95,21 @@ def test_bench_reduces_max_time_and_summed_counts():
         assert p.exitcode == 0
     for _, t, counts in got:  # every rank ends with the same whole-job figures
         assert t == 101.0 and counts == [3, 30]
+
+
+@pytest.mark.parametrize("chunk", [1, 4, 32])
+def test_shard_ranges_partition_any_chunk_and_offset(chunk):
+    import tdfs_b200 as T
+    for begin, end, world in [(0, 100, 3), (600000, 606000, 4), (17, 31, 2), (5, 6, 8)]:
+        seen = []
+        for r in range(world):
+            seen += [e for b, en in T.shard_edge_ranges(end, r, world, chunk, begin) for e in range(b, en)]
+        assert sorted(seen) == list(range(begin, end))
+
+
+def test_bench_deal_chunk():
+    import bench
+    assert bench.deal_chunk(6000, 1) == 0            # one rank: the library decides
+    assert bench.deal_chunk(6000, 2) == 1            # a 1/1000 slice of the power-law graph
+    assert bench.deal_chunk(65646, 2) == 4           # the ER graph of the small configs
+    assert bench.deal_chunk(10 ** 9, 8) == 32
