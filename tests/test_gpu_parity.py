@@ -130,12 +130,20 @@ def test_complete_graph_closed_form(T, n):
             assert got == math.perm(n, k)
 
 
-def test_edge_shards_sum_to_total(er, T):
-    """Level-0 chunks dealt round-robin over shards (the multi-GPU split)."""
+@pytest.mark.parametrize("chunk", [0, 1, 4])
+def test_edge_shards_sum_to_total(er, T, chunk):
+    """Level-0 chunks dealt round-robin over shards (the multi-GPU split), with
+    the default 32-edge deal and with explicit finer chunks, over the whole
+    graph and over a slice; batched launches deal the same way."""
     P = T.PatternPreprocessor(text=CYCLE4)
     total = T.count(er.dev, P).count
-    parts = [T.count(er.dev, P, T.default_options(edge_stride=3, edge_phase=r)).count for r in range(3)]
+    parts = [T.count(er.dev, P, T.shard_options(r, 3, edge_chunk=chunk)).count for r in range(3)]
     assert sum(parts) == total and min(parts) > 0
+    b, e = 1000, 7000
+    part = T.count(er.dev, P, T.default_options(edge_begin=b, edge_end=e)).count
+    shards = [T.count_batch(er.dev, [P], T.shard_options(r, 4, edge_begin=b, edge_end=e, edge_chunk=chunk))[0][0]
+              for r in range(4)]
+    assert sum(shards) == part
 
 
 def test_cli_matches_reference_line_format(T, tmp_path):
