@@ -401,9 +401,9 @@ def admit_stream(T, g, texts, max_matches, max_scanned):
 
 
 def run_serve(args):
-    """Config 5: a stream of random labeled 3-7 vertex queries (density
-    U[0.3, 0.8], labels U[0,4), seed 5) against the labeled power-law graph of
-    config 2 (labels U[0,4), seed 2).  Most such queries on this graph have
+    """The served stream (c5): random labeled 3-7 vertex queries (density
+    U[0.3, 0.8], labels U[0,4), seed 5) against the power-law graph of c2 with
+    labels U[0,4), seed 2.  Most such queries on this graph have
     1e9 to 1e16 matches (sparse 7-vertex patterns around 20k-degree hubs), far
     beyond any DFS in a benchmark; the stream is admitted by estimated work
     (tdfs_estimate) and the admitted queries are run four ways: sequential
