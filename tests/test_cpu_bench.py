@@ -30,3 +30,20 @@ def test_clock_record_without_nvidia_smi():
     c = bench.ClockSampler(0)  # never started
     rec = c.stop()
     assert rec["sm_mhz"] is None and rec["reasons"] == ["nvidia-smi unavailable"]
+
+
+def test_served_stream_admission_by_estimate():
+    """The c5 stream keeps exactly the queries whose estimated count and scan
+    work fit the budget (an impossible pattern always fits, a budget of zero
+    scanned entries admits nothing that scans)."""
+    import tdfs_b200 as T
+    g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
+    none = "v 0 9\nv 1 9\nv 2 9\ne 0 1 1\ne 0 2 1\ne 1 2 1\n"   # label 9 occurs nowhere: 0 matches, 0 scans
+    tri = "v 0 1\nv 1 1\nv 2 1\ne 0 1 1\ne 0 2 1\ne 1 2 1\n"
+    wide = "v 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 1 2 1\ne 1 3 1\n"  # a labeled star: many matches
+    texts = [none, tri, wide]
+    assert bench.admit_stream(T, g, texts, 1e12, 1e12) == [0, 1, 2]
+    assert bench.admit_stream(T, g, texts, 1e12, 0) == [0]
+    est_wide = T.estimate(g, T.PatternPreprocessor(text=wide, labeled=True), 1024, 2).matches
+    assert est_wide > 0
+    assert 2 not in bench.admit_stream(T, g, texts, est_wide / 1000, 1e12)
