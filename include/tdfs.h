@@ -164,9 +164,13 @@ int tdfs_server_destroy(tdfs_server *s); /* drains admitted queries, stops the k
  * library's device image, held on each GPU that uses the library until the
  * process exits.  Graphs whose derived arrays do not fit in it are rejected
  * with TDFS_ERR_CAPACITY (about 4*E + 5*n bytes, up to ~35 MiB, must fit).
- * The first call on a device looks up the array's address; make it before
- * any stream capture.  Calls share the array: calls that overlap on the GPU
- * race, so serialise them.  opt may be NULL; opt->stream is honoured. */
+ * d_colidx must be 16-byte aligned (TDFS_ERR_ARG otherwise): the kernel reads
+ * adjacency windows with 16-byte loads.  When E is not a multiple of 4 those
+ * windows are turned off, so nothing past colidx[E-1] is read.  The first
+ * call on a device looks up the array's address.  A call waits for its
+ * kernel and cannot be recorded into a CUDA graph: on a capturing stream it
+ * returns TDFS_ERR_ARG.  Calls share the array: calls that overlap on the
+ * GPU race, so serialise them.  opt may be NULL; opt->stream is honoured. */
 int tdfs_count_static(int device, int64_t n, int64_t nedges, const int64_t *d_rowptr, const int32_t *d_colidx,
                       const int32_t *d_labels, const tdfs_plan *p, const tdfs_options *opt, uint64_t *count);
 
@@ -178,6 +182,19 @@ int tdfs_csr_view(const tdfs_csr *c, int64_t *n, int64_t *nedges, const int64_t 
 int tdfs_csr_write(const tdfs_csr *c, const char *prefix); /* .label.bin too when labelled */
 int tdfs_csr_set_labels(tdfs_csr *c, int nlabels, uint64_t seed); /* uniform [0, nlabels) */
 int tdfs_csr_free(tdfs_csr *c);
+/* Host CSR from caller arrays (copied; labels may be NULL), checked as
+ * tdfs_graph_from_csr checks them: replaces reading a converted graph back
+ * (src/graph.h:136-193) for graphs already in memory. */
+int tdfs_csr_from_arrays(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx,
+                         const int32_t *labels, tdfs_csr **out);
+/* Descending-degree relabelling of any graph (graph_converter/relabel.cpp:
+ * 11-71): new vertex i is the i-th of the (degree, id) pairs sorted in
+ * descending order, rows re-sorted; labels move with their vertices. */
+int tdfs_csr_relabel(const tdfs_csr *in, tdfs_csr **out);
+/* Degree orientation of any graph (graph_converter/halve.cpp:10-42): edge
+ * (s, d) is kept when deg(d) > deg(s), or they tie and d > s; max_degree
+ * becomes the largest kept row.  Vertex ids and labels are unchanged. */
+int tdfs_csr_halve(const tdfs_csr *in, tdfs_csr **out);
 /* Erdos-Renyi G(n, p), p = avg_degree / (n - 1) */
 int tdfs_gen_er(int64_t n, double avg_degree, uint64_t seed, tdfs_csr **out);
 /* Chung-Lu power law: ~undirected_edges edges, exponent gamma, degree cap,

@@ -24,6 +24,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libtdfs_b200.so")
 BIN_DIR = os.path.join(_HERE, "bin")
+CONVERT = os.path.join(BIN_DIR, "tdfs_convert")  # host-only graph writer / converter
 
 ERR_NAMES = {1: "IO", 2: "FORMAT", 3: "PATTERN", 4: "CUDA", 5: "CAPACITY", 6: "TIMEOUT", 7: "ARG",
              8: "ADMISSION"}
@@ -35,6 +36,7 @@ EXPORTS = [
     "tdfs_plan_compile", "tdfs_plan_from_text", "tdfs_plan_dump", "tdfs_plan_info", "tdfs_plan_free",
     "tdfs_count", "tdfs_count_batch",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
+    "tdfs_csr_from_arrays", "tdfs_csr_relabel", "tdfs_csr_halve",
     "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern", "tdfs_estimate",
     "tdfs_autotune", "tdfs_count_static", "tdfs_server_options_default", "tdfs_server_create", "tdfs_server_submit", "tdfs_server_wait",
     "tdfs_server_stats", "tdfs_server_destroy",
@@ -130,6 +132,9 @@ def lib() -> C.CDLL:
     L.tdfs_csr_write.argtypes = [vp, C.c_char_p]
     L.tdfs_csr_set_labels.argtypes = [vp, ci, C.c_uint64]
     L.tdfs_csr_free.argtypes = [vp]
+    L.tdfs_csr_from_arrays.argtypes = [i64, i64, vp, vp, vp, pp]
+    L.tdfs_csr_relabel.argtypes = [vp, pp]
+    L.tdfs_csr_halve.argtypes = [vp, pp]
     L.tdfs_gen_er.argtypes = [i64, C.c_double, C.c_uint64, pp]
     L.tdfs_gen_chung_lu.argtypes = [i64, i64, C.c_double, i32, C.c_uint64, pp]
     L.tdfs_gen_rmat.argtypes = [ci, ci, C.c_double, C.c_double, C.c_double, C.c_uint64, pp]
@@ -190,10 +195,35 @@ class HostCSR:
     def write(self, prefix: str):
         _check(lib().tdfs_csr_write(self._h, prefix.encode()))
 
+    def relabel(self) -> "HostCSR":
+        """Descending-degree relabelling (graph_converter/relabel.cpp:11-71)."""
+        h = C.c_void_p()
+        _check(lib().tdfs_csr_relabel(self._h, C.byref(h)))
+        return HostCSR(h)
+
+    def halve(self) -> "HostCSR":
+        """Degree orientation: one direction of every edge
+        (graph_converter/halve.cpp:10-42)."""
+        h = C.c_void_p()
+        _check(lib().tdfs_csr_halve(self._h, C.byref(h)))
+        return HostCSR(h)
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.tdfs_csr_free(self._h)
             self._h = None
+
+
+def csr_from_arrays(rowptr, colidx, labels=None) -> HostCSR:
+    """Host CSR copied from arrays (int64 rowptr, int32 colidx, optional
+    int32 labels), checked like the file reader."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.int64)
+    colidx = np.ascontiguousarray(colidx, dtype=np.int32)
+    lab = None if labels is None else np.ascontiguousarray(labels, dtype=np.int32)
+    h = C.c_void_p()
+    _check(lib().tdfs_csr_from_arrays(len(rowptr) - 1, len(colidx), rowptr.ctypes.data, colidx.ctypes.data,
+                                      None if lab is None else lab.ctypes.data, C.byref(h)))
+    return HostCSR(h)
 
 
 def read_csr(prefix: str, labeled: bool = False) -> HostCSR:

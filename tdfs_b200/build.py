@@ -2,7 +2,9 @@
 
     python -m tdfs_b200.build        (or tdfs_b200.build.build())
 
-Outputs: tdfs_b200/lib/libtdfs_b200.so, tdfs_b200/bin/ulb, tdfs_b200/bin/lb.
+Outputs: tdfs_b200/lib/libtdfs_b200.so, tdfs_b200/bin/ulb, tdfs_b200/bin/lb, and
+tdfs_b200/bin/tdfs_convert (the host-only graph writer and converter: no CUDA
+runtime, so processes that only prepare graph files never load the engine).
 nvcc cross-compiles without a GPU; the objects are rebuilt only when a source
 is newer than its output.
 """
@@ -19,10 +21,11 @@ BINDIR = os.path.join(HERE, "bin")
 OBJDIR = os.path.join(HERE, "lib", "obj")
 LIB = os.path.join(LIBDIR, "libtdfs_b200.so")
 NVCC = os.environ.get("NVCC", "nvcc")
+CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall", "--expt-relaxed-constexpr"]
 
-SOURCES = ["plan.cpp", "csr.cpp", "capi.cpp", "serve.cpp", "graph.cu", "match.cu", "static_count.cu", "estimate.cpp"]
+SOURCES = ["error.cpp", "plan.cpp", "csr.cpp", "capi.cpp", "serve.cpp", "graph.cu", "match.cu", "static_count.cu", "estimate.cpp"]
 HEADERS = ["common.h", "plan.h", "csr.h", "graph.h", "match.cuh", "serve.h"]
 
 
@@ -59,6 +62,10 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         if _newer([cli, LIB], out):
             _run([NVCC, *ARCH, "-std=c++17", "-O2", f"-DTDFS_LABELED={lab}", cli, "-o", out,
                   f"-L{LIBDIR}", "-ltdfs_b200", f"-Xlinker=-rpath,$ORIGIN/../lib"], verbose)
+    conv = os.path.join(BINDIR, "tdfs_convert")
+    conv_src = [os.path.join(CSRC, s) for s in ("convert.cpp", "csr.cpp", "error.cpp")]
+    if _newer(conv_src + hdrs, conv):
+        _run([CXX, "-std=c++17", "-O3", "-Wall", "-pthread", *conv_src, "-o", conv], verbose)
     return LIB
 
 

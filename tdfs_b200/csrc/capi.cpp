@@ -7,6 +7,7 @@
 #include <cstring>
 #include <fstream>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -25,29 +26,6 @@ struct tdfs_plan {
 namespace tdfs {
 
 namespace {
-thread_local std::string g_error;
-}
-
-void set_error(const char *fmt, ...) {
-  char buf[1024];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  g_error = buf;
-}
-
-int fail(int code, const char *fmt, ...) {
-  char buf[1024];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  g_error = buf;
-  return code;
-}
-
-namespace {
 
 int cuda_err(cudaError_t e, const char *what) {
   return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
@@ -57,16 +35,23 @@ int cuda_err(cudaError_t e, const char *what) {
 }  // namespace
 
 int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out) {
-  // device properties are queried once per device (the query costs ~ms)
+  // device properties are queried once per device (the query costs ~ms);
+  // host threads that make their first calls at once fill the cache under
+  // the lock, and readers copy the entry out under it
   static cudaDeviceProp props[64];
   static bool have[64] = {};
+  static std::mutex mu;
   if (g->device < 0 || g->device >= 64) return fail(TDFS_ERR_ARG, "device index");
-  if (!have[g->device]) {
-    cudaError_t e = cudaGetDeviceProperties(&props[g->device], g->device);
-    if (e != cudaSuccess) return cuda_err(e, "cudaGetDeviceProperties");
-    have[g->device] = true;
+  cudaDeviceProp prop;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!have[g->device]) {
+      cudaError_t e = cudaGetDeviceProperties(&props[g->device], g->device);
+      if (e != cudaSuccess) return cuda_err(e, "cudaGetDeviceProperties");
+      have[g->device] = true;
+    }
+    prop = props[g->device];
   }
-  const cudaDeviceProp &prop = props[g->device];
   LaunchShape s;
   std::memset(&s, 0, sizeof s);
   s.warps_per_block = o.warps_per_block > 0 ? o.warps_per_block : 8;
@@ -312,8 +297,6 @@ const DevPlan &plan_device_table(const tdfs_plan *p) { return p->dev; }
 using namespace tdfs;
 
 extern "C" {
-
-const char *tdfs_last_error(void) { return g_error.c_str(); }
 
 int tdfs_version(void) { return 1; }
 

@@ -141,11 +141,120 @@ void csr_from_pairs(int64_t n, std::vector<std::pair<uint32_t, uint32_t>> &pairs
   out->max_degree = md;
 }
 
+// Descending-degree relabelling as graph_converter/relabel.cpp:27-58 does
+// it: (degree, id) pairs sorted with std::greater, so ties go to the larger
+// old id first; vertex i of the output is order[i] of the input, every row
+// is mapped through the new ids and sorted again.  Labels move with their
+// vertices.
+void relabel_by_degree(const tdfs_csr &g, tdfs_csr *c) {
+  const int64_t n = g.n;
+  std::vector<std::pair<int64_t, int64_t>> order(n);
+  for (int64_t v = 0; v < n; ++v) order[v] = {g.rowptr[v + 1] - g.rowptr[v], v};
+  std::sort(order.begin(), order.end(), std::greater<>());
+  std::vector<int32_t> newid(n);
+  for (int64_t i = 0; i < n; ++i) newid[order[i].second] = (int32_t)i;
+  c->n = n;
+  c->nedges = g.nedges;
+  c->max_degree = g.max_degree;
+  c->rowptr.assign(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) c->rowptr[i + 1] = c->rowptr[i] + order[i].first;
+  c->colidx.resize(g.nedges);
+  parallel_for(n, [&](int64_t b, int64_t e) {
+    for (int64_t i = b; i < e; ++i) {
+      int64_t old = order[i].second;
+      int32_t *dst = c->colidx.data() + c->rowptr[i];
+      int64_t d = g.rowptr[old + 1] - g.rowptr[old];
+      for (int64_t t = 0; t < d; ++t) dst[t] = newid[g.colidx[g.rowptr[old] + t]];
+      std::sort(dst, dst + d);
+    }
+  });
+  c->labels.clear();
+  if (!g.labels.empty()) {
+    c->labels.resize(n);
+    for (int64_t i = 0; i < n; ++i) c->labels[i] = g.labels[order[i].second];
+  }
+}
+
+// Degree orientation as graph_converter/halve.cpp:17-32 does it: edge (s, d)
+// is kept when deg(d) > deg(s), or the degrees tie and d > s, so each
+// undirected edge of a symmetric graph survives in exactly one direction.
+// Rows stay sorted; vertex ids and labels are unchanged.
+void halve_by_degree(const tdfs_csr &g, tdfs_csr *c) {
+  const int64_t n = g.n;
+  auto deg = [&](int64_t v) { return g.rowptr[v + 1] - g.rowptr[v]; };
+  std::vector<int64_t> keep(n, 0);
+  parallel_for(n, [&](int64_t b, int64_t e) {
+    for (int64_t s = b; s < e; ++s) {
+      const int64_t ds = deg(s);
+      int64_t k = 0;
+      for (int64_t j = g.rowptr[s]; j < g.rowptr[s + 1]; ++j) {
+        const int64_t d = g.colidx[j], dd = deg(d);
+        k += dd > ds || (dd == ds && d > s);
+      }
+      keep[s] = k;
+    }
+  });
+  c->n = n;
+  c->rowptr.assign(n + 1, 0);
+  int64_t md = 0;
+  for (int64_t v = 0; v < n; ++v) {
+    c->rowptr[v + 1] = c->rowptr[v] + keep[v];
+    md = std::max(md, keep[v]);
+  }
+  c->nedges = c->rowptr[n];
+  c->max_degree = (int32_t)md;
+  c->colidx.resize(c->nedges);
+  parallel_for(n, [&](int64_t b, int64_t e) {
+    for (int64_t s = b; s < e; ++s) {
+      const int64_t ds = deg(s);
+      int32_t *out = c->colidx.data() + c->rowptr[s];
+      for (int64_t j = g.rowptr[s]; j < g.rowptr[s + 1]; ++j) {
+        const int64_t d = g.colidx[j], dd = deg(d);
+        if (dd > ds || (dd == ds && d > s)) *out++ = (int32_t)d;
+      }
+    }
+  });
+  c->labels = g.labels;
+}
+
 }  // namespace tdfs
 
 using namespace tdfs;
 
 extern "C" {
+
+int tdfs_csr_from_arrays(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx,
+                         const int32_t *labels, tdfs_csr **out) {
+  if (!rowptr || (!colidx && nedges) || !out) return fail(TDFS_ERR_ARG, "null argument");
+  int32_t md = 0;
+  int rc = validate_csr(n, nedges, rowptr, colidx, &md);
+  if (rc) return rc;
+  auto *c = new tdfs_csr;
+  c->n = n;
+  c->nedges = nedges;
+  c->max_degree = md;
+  c->rowptr.assign(rowptr, rowptr + n + 1);
+  c->colidx.assign(colidx, colidx + nedges);
+  if (labels) c->labels.assign(labels, labels + n);
+  *out = c;
+  return TDFS_OK;
+}
+
+int tdfs_csr_relabel(const tdfs_csr *in, tdfs_csr **out) {
+  if (!in || !out) return fail(TDFS_ERR_ARG, "null argument");
+  auto *c = new tdfs_csr;
+  relabel_by_degree(*in, c);
+  *out = c;
+  return TDFS_OK;
+}
+
+int tdfs_csr_halve(const tdfs_csr *in, tdfs_csr **out) {
+  if (!in || !out) return fail(TDFS_ERR_ARG, "null argument");
+  auto *c = new tdfs_csr;
+  halve_by_degree(*in, c);
+  *out = c;
+  return TDFS_OK;
+}
 
 int tdfs_csr_read(const char *prefix, int labeled, tdfs_csr **out) {
   if (!prefix || !out) return fail(TDFS_ERR_ARG, "null argument");
@@ -296,28 +405,8 @@ int tdfs_gen_chung_lu(int64_t n, int64_t m, double gamma, int32_t cap, uint64_t 
   }
   tdfs_csr g;
   csr_from_pairs(n, pairs, &g);
-  // relabel by descending degree
-  std::vector<std::pair<int64_t, int64_t>> order(n);
-  for (int64_t v = 0; v < n; ++v) order[v] = {g.rowptr[v + 1] - g.rowptr[v], v};
-  std::sort(order.begin(), order.end(), std::greater<>());
-  std::vector<int32_t> newid(n);
-  for (int64_t i = 0; i < n; ++i) newid[order[i].second] = (int32_t)i;
   auto *c = new tdfs_csr;
-  c->n = n;
-  c->nedges = g.nedges;
-  c->max_degree = g.max_degree;
-  c->rowptr.assign(n + 1, 0);
-  for (int64_t i = 0; i < n; ++i) c->rowptr[i + 1] = c->rowptr[i] + order[i].first;
-  c->colidx.resize(g.nedges);
-  parallel_for(n, [&](int64_t b, int64_t e) {
-    for (int64_t i = b; i < e; ++i) {
-      int64_t old = order[i].second;
-      int32_t *dst = c->colidx.data() + c->rowptr[i];
-      int64_t d = g.rowptr[old + 1] - g.rowptr[old];
-      for (int64_t t = 0; t < d; ++t) dst[t] = newid[g.colidx[g.rowptr[old] + t]];
-      std::sort(dst, dst + d);
-    }
-  });
+  relabel_by_degree(g, c);
   *out = c;
   return TDFS_OK;
 }

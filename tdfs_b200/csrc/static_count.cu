@@ -23,12 +23,24 @@
 // whose work overlaps on the GPU (different streams or host threads) race on
 // the array; callers must serialise them.
 //
+// colidx must start on a 16-byte boundary: the kernel stages adjacency
+// windows with 16-byte vector loads at offsets rounded down to 4 ints, and a
+// misaligned base would fault.  Such a pointer (a sub-allocation, a slice
+// like colidx + 1) is rejected with TDFS_ERR_ARG before any GPU work.  The
+// same loads round the end of a window up to 4 ints, so when E is not a
+// multiple of 4 they could read up to 3 ints past colidx[E-1], outside the
+// caller's buffer; for those graphs the staged windows are turned off (the
+// kernel searches the lists directly; the count is the same).
+//
 // The first call on each device looks up the array's device address
-// (cudaGetSymbolAddress, with that device current); make that first call
-// before starting any stream capture.
+// (cudaGetSymbolAddress, with that device current).  The call copies its
+// query record from host stack memory and waits for the kernel, so it cannot
+// be recorded into a CUDA graph: a call on a stream that is being captured
+// is rejected with TDFS_ERR_ARG.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -81,6 +93,8 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   if (!d_rowptr || (!d_colidx && nedges) || !p || !count) return fail(TDFS_ERR_ARG, "null argument");
   if (device < 0 || device >= kMaxDevices) return fail(TDFS_ERR_ARG, "device %d out of range", device);
   if (n < 0 || n > INT32_MAX - 1 || nedges < 0) return fail(TDFS_ERR_ARG, "bad graph size");
+  if (reinterpret_cast<uintptr_t>(d_colidx) & 15)
+    return fail(TDFS_ERR_ARG, "colidx must be 16-byte aligned (the kernel reads it with 16-byte vector loads)");
   const DevPlan &plan = plan_device_table(p);
   if (plan.labeled && !d_labels) return fail(TDFS_ERR_ARG, "labeled pattern without vertex labels");
   const Layout L = layout(n, nedges);
@@ -104,6 +118,16 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   tdfs_options o;
   if (opt) o = *opt; else tdfs_options_default(&o);
   cudaStream_t st = static_cast<cudaStream_t>(o.stream);
+  {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cs);
+    if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "cudaStreamIsCapturing: %s", cudaGetErrorString(e));
+    if (cs != cudaStreamCaptureStatusNone)
+      return fail(TDFS_ERR_ARG, "tdfs_count_static cannot be called on a stream that is being captured");
+  }
+  // 16-byte window loads may round the last list's end up to 4 ints: without
+  // that slack after colidx[E-1], search the lists directly instead
+  if (nedges % 4 != 0) o.merge_window = -1;
   RunCtl *ctl = reinterpret_cast<RunCtl *>(base + L.ctl);
   SplitUnit *units = reinterpret_cast<SplitUnit *>(base + L.units);
   QueueHdr *qh = reinterpret_cast<QueueHdr *>(base + L.qhdr);

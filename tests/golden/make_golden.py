@@ -1,7 +1,10 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py plans        # in the build container
+    python tests/golden/make_golden.py plans --reference <reference checkout>
     python tests/golden/make_golden.py ref-counts   # on a GPU box
+
+(``--reference`` may also come from the TDFS_REFERENCE environment variable;
+it is the checkout whose data/pattern/*.g are recorded.)
 
 ``plans``: runs the reference's own PatternPreprocessor (src/pattern.h, with
 bliss compiled from its sources; see oracle/Makefile target ``ref``) through
@@ -28,7 +31,17 @@ import tempfile
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), "..", ".."))
 sys.path.insert(0, ROOT)
-REF_PATTERNS = "/root/reference/data/pattern"
+
+def ref_patterns_dir() -> str:
+    """data/pattern of the reference checkout named by --reference or the
+    TDFS_REFERENCE environment variable."""
+    ref = os.environ.get("TDFS_REFERENCE")
+    if "--reference" in sys.argv:
+        ref = sys.argv[sys.argv.index("--reference") + 1]
+    if not ref:
+        raise SystemExit("give the reference checkout: --reference <dir> or TDFS_REFERENCE=<dir>")
+    return os.path.join(ref, "data", "pattern")
+
 REFBIN = os.path.join(ROOT, "oracle", "_ref")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
@@ -70,7 +83,7 @@ def refdump(text: str, labeled: bool) -> dict:
 def make_plans():
     cases = []
     for i in range(1, 15):
-        with open(os.path.join(REF_PATTERNS, f"{i}.g")) as f:
+        with open(os.path.join(ref_patterns_dir(), f"{i}.g")) as f:
             cases.append((f"ref/{i}.g", f.read()))
     cases += [("triangle", TRIANGLE), ("cycle4", CYCLE4), ("house", HOUSE), ("odd_labels", ODD_LABELS),
               ("zero_edge", ZERO_EDGE)]

@@ -28,6 +28,5 @@ def reference_patterns():
     return out
 
 
-DIAMOND = None  # ref/1.g
 K4 = clique(4)
 K5 = clique(5)

@@ -102,3 +102,78 @@ def test_pattern_generator(T):
         p = T.PatternPreprocessor(text=text, labeled=True)  # compiles: connected order
         d = p.dump()
         assert d["k"] == k and 1 in d["backward_neighbors"][2]
+
+
+def _edges(g):
+    src = np.repeat(np.arange(g.n), np.diff(g.rowptr))
+    return set(zip(src.tolist(), g.colidx.tolist()))
+
+
+def test_relabel_any_graph(T):
+    """Descending-degree relabelling (graph_converter/relabel.cpp:27-58):
+    (degree, id) pairs sorted in descending order give the new ids, so the
+    result is an isomorphic copy whose degrees never increase and whose
+    ties keep the larger old id first; labels move with their vertices."""
+    g = T.gen_rmat(10, 8, 0.57, 0.19, 0.19, 9).set_labels(5, 3)
+    r = g.relabel()
+    deg = np.diff(g.rowptr)
+    order = sorted(range(g.n), key=lambda v: (deg[v], v), reverse=True)
+    new = np.empty(g.n, np.int64)
+    new[order] = np.arange(g.n)
+    assert r.n == g.n and r.nedges == g.nedges and r.max_degree == g.max_degree
+    assert (np.diff(np.diff(r.rowptr)) <= 0).all()
+    assert _edges(r) == {(int(new[a]), int(new[b])) for a, b in _edges(g)}
+    assert (r.labels[new] == g.labels).all()
+    for v in range(r.n):
+        assert (np.diff(r.colidx[r.rowptr[v]:r.rowptr[v + 1]]) > 0).all()
+    # the Chung-Lu generator relabels with the same rule: a second pass only
+    # permutes equal-degree ties, and the degree sequence is unchanged
+    c = T.gen_chung_lu(5000, 15000, 2.1, 300, 1)
+    assert (np.diff(c.relabel().rowptr) == np.diff(c.rowptr)).all()
+
+
+def test_halve_any_graph(T):
+    """Degree orientation (graph_converter/halve.cpp:17-32): every undirected
+    edge survives once, towards the higher-degree end (the larger id on a
+    tie); symmetrising the result gives the graph back."""
+    g = T.gen_chung_lu(5000, 15000, 2.1, 300, 1).set_labels(4, 2)
+    h = g.halve()
+    deg = np.diff(g.rowptr)
+    he = _edges(h)
+    assert h.nedges * 2 == g.nedges and len(he) == h.nedges
+    assert all(deg[d] > deg[s] or (deg[d] == deg[s] and d > s) for s, d in he)
+    assert he | {(d, s) for s, d in he} == _edges(g)
+    assert h.max_degree == np.diff(h.rowptr).max() and (h.labels == g.labels).all()
+
+
+def test_csr_from_arrays_checks_rows(T):
+    g = T.gen_er(300, 6.0, 1)
+    c = T.csr_from_arrays(g.rowptr, g.colidx)
+    assert (c.colidx == g.colidx).all() and c.max_degree == g.max_degree
+    bad = g.colidx.copy()
+    bad[g.rowptr[3]:g.rowptr[4]] = bad[g.rowptr[3]:g.rowptr[4]][::-1]
+    with pytest.raises(T.TdfsError) as e:
+        T.csr_from_arrays(g.rowptr, bad)
+    assert e.value.code == 2
+
+
+def test_convert_tool_writes_the_generators_graphs(T, tmp_path):
+    """tdfs_convert (host-only, no CUDA runtime) writes the same files as the
+    library's generators, and relabel/halve on disk match the C ABI."""
+    import subprocess
+    pre = str(tmp_path / "er")
+    subprocess.run([T.CONVERT, "er", "4096", "16", "0", pre], check=True, capture_output=True)
+    subprocess.run([T.CONVERT, "labels", pre, "4", "2"], check=True, capture_output=True)
+    g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
+    r = T.read_csr(pre, labeled=True)
+    assert (r.rowptr == g.rowptr).all() and (r.colidx == g.colidx).all() and (r.labels == g.labels).all()
+    for step, fn in (("relabel", g.relabel), ("halve", g.halve)):
+        out = str(tmp_path / step)
+        subprocess.run([T.CONVERT, step, pre, out], check=True, capture_output=True)
+        a, b = T.read_csr(out, labeled=True), fn()
+        assert (a.rowptr == b.rowptr).all() and (a.colidx == b.colidx).all() and (a.labels == b.labels).all()
+    cl = str(tmp_path / "cl")
+    subprocess.run([T.CONVERT, "cl", "20000", "60000", "2.1", "600", "1", cl], check=True, capture_output=True)
+    assert (T.read_csr(cl).colidx == T.gen_chung_lu(20000, 60000, 2.1, 600, 1).colidx).all()
+    bad = subprocess.run([T.CONVERT, "halve", str(tmp_path / "missing"), out], capture_output=True, text=True)
+    assert bad.returncode == 1 and "cannot open" in bad.stderr

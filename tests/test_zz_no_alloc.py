@@ -101,3 +101,29 @@ def test_static_rejects_graphs_beyond_the_array(T):
         with pytest.raises(T.TdfsError) as ei:
             T.count_static(0, n, e, fake, fake, None, P)
         assert ei.value.code == CAPACITY and "scratch" in str(ei.value)
+
+
+def test_static_rejects_misaligned_colidx(T):
+    """colidx is read with 16-byte vector loads: a pointer off a 16-byte
+    boundary (a slice such as colidx + 1) is refused before any CUDA call
+    (runs without a GPU: the pointers are never dereferenced)."""
+    P = T.PatternPreprocessor(text=TRIANGLE)
+    for off in (4, 8, 12):
+        with pytest.raises(T.TdfsError) as ei:
+            T.count_static(0, 100, 400, 256, 256 + off, None, P)
+        assert ei.value.code == 7 and "aligned" in str(ei.value)
+
+
+@pytest.mark.gpu
+def test_static_edge_count_not_multiple_of_four(T):
+    """A graph whose E is not a multiple of 4, its colidx in a buffer of
+    exactly E ints: the count still equals tdfs_count."""
+    import torch
+    csr = T.gen_er(1001, 7.0, 3)
+    assert csr.nedges % 4 != 0
+    dev = _device_csr(csr)
+    for text in (TRIANGLE, CYCLE4, HOUSE):
+        P = T.PatternPreprocessor(text=text)
+        want = T.count(T.GraphPreprocessor(csr=csr), P).count
+        assert _static(T, csr, dev, P) == want
+    torch.cuda.synchronize()
