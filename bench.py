@@ -1,35 +1,56 @@
 #!/usr/bin/env python
 """Benchmark of the subgraph-counting hot path (matches/s).
 
-    python bench.py [--gpus N --steps K --warmup W] [--workload c2] [--impl tdfs|reference]
+    python bench.py [--gpus N --steps K --warmup W] [--workload c13|c1|c2|c3|c4|c5]
+                    [--impl tdfs|reference] [--no-c2]
 
-One step = every pattern of the workload counted over one batch of level-0
-edges in one batched launch (tdfs_count_batch), the graph already resident in
-HBM: the whole edge array for the small
-configs (c1, c3), one contiguous 1/1000 slice of it for the power-law config
-(c2; its house count is ~1e13 matches, about 25 GPU-minutes for the whole
-graph) and a 1/500000 slice for the scale-24 R-MAT graph (c4; its 6-clique
-count is ~4e18), the timed slices spread evenly over the array.  c5 is the
-served stream of random labeled queries.  With N ranks (torchrun, one
-process per GPU) the level-0 edge chunks of each step are dealt round-robin
-over the ranks (strong scaling, one u64 all-reduce per step).
+Default workload (c13): the small configs together.  The graph is Erdos-Renyi,
+n=4096, average degree 16, seed 0, with vertex labels uniform in [0,4) (seed 2).
+One step counts 12 patterns over the whole graph:
+- the four unlabeled patterns of config 1 (triangle, 4-cycle, diamond, 4-clique);
+- the eight labeled 6-7 vertex random patterns of config 3.
 
-The JSON line reports
-  value       matches/s of the device-timed steps (CUDA events, max over ranks)
-  e2e         the same metric through the public C ABI with host buffers:
-              graph upload from pinned host memory + counts + read-back
-  roofline    merge-model algorithmic bytes per match-kernel launch / mean
-              launch time, against the measured HBM copy bandwidth
-  cpu_baseline the multithreaded CPU oracle on a bounded prefix of a step
-  clocks      nvidia-smi SM clocks and throttle reasons sampled while timing
+Every pattern of a step runs in one batched persistent launch per mode
+(tdfs_count_batch): unlabeled and labeled.  The launch knobs come from the
+autotuner (tdfs_autotune), run once before the timed steps.  Launches replay a
+captured CUDA graph.
 
---impl reference runs the reference's own CUDA kernel (built from the
-reference sources for sm_100a into oracle/_ref/) on the same graph, written in
-its file format, over the same edge ranges, reading its own kernel timing.
+The power-law config (c2) is carried as a sub-record of the default line (skip
+it with --no-c2):
+- the 5-clique over the whole graph in one launch;
+- the house over five fixed 1/1000 slices of the level-0 edge array.  Its
+  whole-graph count is ~1e13 matches, about 25 GPU-minutes.
+`--workload c2` times slices of the edge array as steps.  `--workload c4`
+does the same on the scale-24 R-MAT graph.  `--workload c5` serves the
+query stream.
+
+With N ranks (torchrun, one process per GPU), the level-0 edge chunks of each
+step are dealt round-robin over the ranks.  This is strong scaling, with one
+u64 all-reduce per step.
+
+The JSON line reports:
+- value: matches/s of the device-timed steps (CUDA events around each step,
+  max over ranks);
+- e2e: the same metric through the public C ABI from pinned host buffers.
+  Each step uploads the graph, compiles the patterns, counts, reads back and
+  frees;
+- roofline: exact merge-model algorithmic bytes per match-kernel launch
+  (from the oracle over the same steps) / mean kernel time, against the
+  measured HBM copy bandwidth;
+- cpu_baseline: the multithreaded CPU oracle on the same work;
+- clocks: nvidia-smi SM clocks and throttle reasons sampled while timing.
+Every count is compared with the CPU oracle before a line is printed.
+
+--impl reference runs the reference's own CUDA kernel.  It is built from the
+reference sources for sm_100a into oracle/_ref/ and driven by refshard.  It
+runs on the same graph, written in its file format by the host-only
+tdfs_convert tool, and on the same steps.  It reads its own kernel timing.
+That process never loads this repository's engine.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -42,13 +63,15 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-import numpy as np  # noqa: E402
-
 TRIANGLE = "# triangle\nv 0 1\nv 1 1\nv 2 1\ne 0 1 1\ne 0 2 1\ne 1 2 1\n"
 CYCLE4 = "# 4-cycle\nv 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 1 2 1\ne 2 3 1\ne 0 3 1\n"
 DIAMOND = "# diamond: 4-cycle plus one chord\nv 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 0 2 1\ne 0 3 1\ne 1 2 1\ne 1 3 1\n"
 HOUSE = ("# house\nv 0 1\nv 1 1\nv 2 1\nv 3 1\nv 4 1\n"
          "e 0 1 1\ne 0 2 1\ne 1 2 1\ne 1 3 1\ne 2 4 1\ne 3 4 1\n")
+CONVERT = os.path.join(ROOT, "tdfs_b200", "bin", "tdfs_convert")
+ORACLE_CLI = os.path.join(ROOT, "oracle", "_build", "oracle_count")
+C2_HOUSE_SLICES = (100, 300, 500, 700, 900)  # of 1000: the c2 sub-record's house slices
+FLUSH_BYTES = 256 << 20  # > the 126 MB L2
 
 
 def clique(k):
@@ -56,37 +79,86 @@ def clique(k):
         f"e {i} {j} 1\n" for i in range(k) for j in range(i + 1, k))
 
 
-def workload(name, T):
-    """(description, host CSR, [(pattern name, text)], labeled, slices).
+# ---- workloads: graph recipe + patterns, shared by both arms ----------------
+
+GRAPHS = {
+    "er": ("er", "4096", "16", "0"),
+    "er_l": ("er", "4096", "16", "0"),
+    "cl": ("cl", "1100000", "3000000", "2.1", "30000", "1"),
+    "rmat": ("rmat", "24", "16", "0.57", "0.19", "0.19", "4"),
+}
+GRAPH_LABELS = {"er_l": (4, 2)}
+
+
+def c3_pattern_specs():
+    """The eight labeled patterns of config 3: random connected 6-7 vertex
+    graphs, edge density 0.4, labels U[0,4), seeds 3000..3007."""
+    return [(6 + i % 2, 0.4, 4, 3000 + i) for i in range(8)]
+
+
+def workload(name):
+    """(description, graph key, [(pattern name, text or spec, labeled)], slices).
 
     slices = S: one step counts every pattern over one contiguous 1/S slice of
-    the level-0 directed-edge array (S = 1: the whole graph)."""
+    the level-0 directed-edge array (S = 1: the whole graph).  A pattern given
+    as a tuple is a tdfs_gen_pattern spec (k, density, nlabels, seed)."""
+    c1 = [("triangle", TRIANGLE, False), ("4-cycle", CYCLE4, False), ("diamond", DIAMOND, False),
+          ("4-clique", clique(4), False)]
+    c3 = [(f"labeled-{i}", spec, True) for i, spec in enumerate(c3_pattern_specs())]
+    er = "ER n=4096 avg-degree 16 seed 0"
+    if name == "c13":
+        return (f"{er}, labels U[0,4) seed 2; config 1's triangle, 4-cycle, diamond, 4-clique (unlabeled) and "
+                "config 3's 8 random 6-7 vertex labeled patterns (density 0.4, seeds 3000-3007); one step = all 12 "
+                "patterns over the whole graph", "er_l", c1 + c3, 1)
     if name == "c1":
-        g = T.gen_er(4096, 16.0, 0)
-        pats = [("triangle", TRIANGLE), ("4-cycle", CYCLE4), ("diamond", DIAMOND), ("4-clique", clique(4))]
-        return ({"workload": "ER n=4096 avg-degree 16 seed 0; triangle, 4-cycle, diamond, 4-clique; "
-                             "one step = every pattern over the whole graph"}, g, pats, False, 1)
-    if name == "c2":
-        g = T.gen_chung_lu(1_100_000, 3_000_000, 2.1, 30_000, 1)
-        pats = [("5-clique", clique(5)), ("house", HOUSE)]
-        return ({"workload": "Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1, degree-ordered ids; 5-clique and "
-                             "house; one step = both patterns over one contiguous 1/1000 slice of the level-0 "
-                             "edge array, timed slices spread evenly over the array"}, g, pats, False, 1000)
+        return (f"{er}; triangle, 4-cycle, diamond, 4-clique; one step = every pattern over the whole graph",
+                "er", c1, 1)
     if name == "c3":
-        g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
-        pats = [(f"labeled-{i}", T.gen_pattern(6 + i % 2, 0.4, 4, 3 * 1000 + i)) for i in range(8)]
-        return ({"workload": "ER n=4096 avg-degree 16 seed 0, labels U[0,4) seed 2; 8 random 6-7 vertex labeled "
-                             "patterns (density 0.4, seed 3); one step = every pattern over the whole graph"},
-                g, pats, True, 1)
+        return (f"{er}, labels U[0,4) seed 2; 8 random 6-7 vertex labeled patterns (density 0.4, seeds "
+                "3000-3007); one step = every pattern over the whole graph", "er_l", c3, 1)
+    if name == "c2":
+        return ("Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1, degree-ordered ids; 5-clique and house; one step "
+                "= both patterns over one contiguous 1/1000 slice of the level-0 edge array, timed slices spread "
+                "evenly over the array", "cl", [("5-clique", clique(5), False), ("house", HOUSE, False)], 1000)
     if name == "c4":
-        # whole-graph counts (estimated): 4-clique ~2e13, 6-clique ~4e18 -- a step is a slice
-        g = T.gen_rmat(24, 16, 0.57, 0.19, 0.19, 4)
-        pats = [("4-clique", clique(4)), ("6-clique", clique(6))]
-        return ({"workload": "R-MAT scale 24 edge-factor 16 a=0.57 b=c=0.19 seed 4, deduplicated and symmetrised "
-                             f"(n={g.n}, {g.nedges} directed edges, max degree {g.max_degree}); 4-clique and "
-                             "6-clique; one step = both patterns over one contiguous 1/500000 slice of the "
-                             "level-0 edge array, timed slices spread evenly over the array"}, g, pats, False, 500000)
+        return ("R-MAT scale 24 edge-factor 16 a=0.57 b=c=0.19 seed 4, deduplicated and symmetrised; 4-clique and "
+                "6-clique; one step = both patterns over one contiguous 1/500000 slice of the level-0 edge array, "
+                "timed slices spread evenly over the array", "rmat",
+                [("4-clique", clique(4), False), ("6-clique", clique(6), False)], 500000)
     raise SystemExit(f"unknown workload {name}")
+
+
+def graph_via_library(T, key):
+    """The workload's graph from the engine's own generators (this arm)."""
+    a = GRAPHS[key]
+    if a[0] == "er":
+        g = T.gen_er(int(a[1]), float(a[2]), int(a[3]))
+    elif a[0] == "cl":
+        g = T.gen_chung_lu(int(a[1]), int(a[2]), float(a[3]), int(a[4]), int(a[5]))
+    else:
+        g = T.gen_rmat(int(a[1]), int(a[2]), float(a[3]), float(a[4]), float(a[5]), int(a[6]))
+    if key in GRAPH_LABELS:
+        g.set_labels(*GRAPH_LABELS[key])
+    return g
+
+
+def graph_via_convert(key, prefix):
+    """The same graph written in the reference's file format by the host-only
+    tdfs_convert tool (no CUDA runtime, no engine library).  Returns E."""
+    out = subprocess.run([CONVERT, *GRAPHS[key], prefix], capture_output=True, text=True, check=True).stdout
+    if key in GRAPH_LABELS:
+        nl, seed = GRAPH_LABELS[key]
+        subprocess.run([CONVERT, "labels", prefix, str(nl), str(seed)], capture_output=True, check=True)
+    return int(out.split()[1])
+
+
+def pattern_text(spec, gen):
+    return spec if isinstance(spec, str) else gen(*spec)
+
+
+def convert_pattern(k, density, nlabels, seed):
+    return subprocess.run([CONVERT, "pattern", str(k), str(density), str(nlabels), str(seed)],
+                          capture_output=True, text=True, check=True).stdout
 
 
 def step_ranges(nedges, slices, steps, warmup):
@@ -184,14 +256,28 @@ def reduce_over_ranks(dist, seconds_or_ms, counts, device="cuda"):
     return float(t.item()), [int(v) for v in m.tolist()]
 
 
-def measured_traffic(workload):
-    """DRAM bytes per timed match-kernel launch of this workload from the ncu
-    capture summarised in profiles/match_kernel_traffic.json, or None."""
+def kernel_source_digest():
+    """SHA-256 (first 16 hex digits) of the match kernel's sources: an ncu
+    record of its traffic holds for the kernel it was captured on."""
+    h = hashlib.sha256()
+    for f in ("match.cu", "match.cuh", "graph.h", "common.h"):
+        with open(os.path.join(ROOT, "tdfs_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
+
+
+def measured_profile(workload, path=None):
+    """The ncu record of the match kernel on this workload
+    (profiles/match_kernel_ncu.json), or None when it was captured on other
+    kernel sources than the ones built here."""
     try:
-        with open(os.path.join(ROOT, "profiles", "match_kernel_traffic.json")) as f:
-            return json.load(f)[workload]["dram_bytes_per_launch"]
+        with open(path or os.path.join(ROOT, "profiles", "match_kernel_ncu.json")) as f:
+            rec = json.load(f)[workload]
     except (OSError, KeyError, ValueError):
         return None
+    if rec.get("kernel_sources") != kernel_source_digest():
+        return None
+    return rec
 
 
 def measured_hbm_peak():
@@ -202,21 +288,30 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def cpu_baseline(g, pats, labeled, rng, budget_s=12.0):
-    """The CPU oracle (multithreaded DFS, same plan and semantics) on a
-    bounded sample of the first timed step: for each pattern, growing prefixes
-    of that step's edge range until about budget_s / len(pats) seconds are
-    spent.  Returns (record, {pattern: (model bytes, matches)})."""
+# ---- the CPU oracle: counts, exact model bytes, CPU baseline -----------------
+
+def oracle_pass(g, pats, ranges, threads=0, budget_s=None):
+    """The CPU oracle over the given level-0 edge ranges for every pattern.
+    Returns ({pattern: (count, merge-model bytes)}, seconds).  With budget_s,
+    the ranges of a pattern are cut to growing prefixes of the first range
+    until that pattern's share of the budget is spent (edge costs vary by
+    orders of magnitude on power-law graphs); the prefixes are returned."""
     from oracle import pyoracle as po
-    G = po.Graph(g.rowptr, g.colidx, g.labels if labeled else None)
-    threads = os.cpu_count() or 1
-    b0, e0 = rng
-    per = {}
-    total = 0
-    spent = 0.0
-    done_edges = []
-    for name, text in pats:
-        P = po.Plan(text, labeled)
+    labeled_any = any(lab for _, _, lab in pats)
+    G = po.Graph(g.rowptr, g.colidx, g.labels if labeled_any else None)
+    out, spent, prefixes = {}, 0.0, {}
+    for name, text, lab in pats:
+        P = po.Plan(text, lab)
+        if budget_s is None:
+            t0 = time.perf_counter()
+            c = b = 0
+            for lo, hi in ranges:
+                cc, bb = po.count(G, P, threads, lo, hi, with_bytes=True)
+                c, b = c + cc, b + bb
+            spent += time.perf_counter() - t0
+            out[name] = (c, b)
+            continue
+        b0, e0 = ranges[0]
         lo, span, byts, cnt, t_pat = b0, 4, 0, 0, 0.0
         share = budget_s / len(pats)
         while lo < e0 and t_pat < share:
@@ -227,56 +322,96 @@ def cpu_baseline(g, pats, labeled, rng, budget_s=12.0):
             t_pat += dt
             cnt += c
             byts += nb
-            # next prefix: double it, but aim at half the time left at this
-            # chunk's rate (edge costs vary by orders of magnitude)
             per_edge = dt / max(1, hi - lo)
             lo, span = hi, max(1, min(span * 2, int(0.5 * (share - t_pat) / max(per_edge, 1e-9))))
-        per[name] = (byts, cnt)
-        total += cnt
+        out[name] = (cnt, byts)
+        prefixes[name] = (b0, lo)
         spent += t_pat
-        done_edges.append(f"{name}: edges [{b0}, {lo})")
-    return ({"value": total / spent if spent > 0 else None, "unit": "matches/s", "cores": threads, "kind": "port",
-             "sample": "CPU oracle, all host threads, on prefixes of the first timed step's edge range (" +
-                       "; ".join(done_edges) + ")", "seconds": round(spent, 2)}, per)
+    return out, spent, prefixes
+
+
+class CountMismatch(RuntimeError):
+    pass
 
 
 def run_tdfs(args, rank, world, dist):
+    import numpy as np
     import torch
     import tdfs_b200 as T
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    desc, g, pats, labeled, slices = workload(args.workload, T)
-    G = T.GraphPreprocessor(csr=g, labeled=labeled, device=dev)
-    plans = [(n, T.PatternPreprocessor(text=t, labeled=labeled)) for n, t in pats]
+    desc, gkey, spec, slices = workload(args.workload)
+    g = graph_via_library(T, gkey)
+    pats = [(n, pattern_text(s, T.gen_pattern), lab) for n, s, lab in spec]
+    labeled_any = any(lab for _, _, lab in pats)
+    G = T.GraphPreprocessor(csr=g, labeled=labeled_any, device=dev)
+    plans = [T.PatternPreprocessor(text=t, labeled=lab) for _, t, lab in pats]
     warm_r, timed_r = step_ranges(g.nedges, slices, args.steps, args.warmup)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
 
-    def opts(rng):
-        return T.shard_options(rank, world, edge_begin=rng[0], edge_end=rng[1],
-                               edge_chunk=deal_chunk(rng[1] - rng[0], world))
+    # launch knobs: the autotuner once, untimed, on every 4th level-0 chunk of
+    # a step; kept when it beats the defaults over whole warm-up steps
+    def shard(rng, base):
+        o = T.Options()
+        for f, _ in T.Options._fields_:
+            setattr(o, f, getattr(base, f))
+        o.edge_begin, o.edge_end = rng
+        o.edge_stride, o.edge_phase = world, rank
+        if world > 1:  # every rank deals the same chunks
+            o.edge_chunk = deal_chunk(rng[1] - rng[0], world)
+        return o
 
-    def step(graph, rng):
-        # every pattern of the step in one persistent launch (tdfs_count_batch)
-        return T.count_batch(graph, [p for _, p in plans], opts(rng))
+    default = T.default_options()
+    tune_range = warm_r[0] if warm_r else timed_r[0]
+    launch = {"autotune": "off"}
+    knobs = default
+    if not args.no_autotune:
+        t0 = time.perf_counter()
+        tuned, sample_ms = T.autotune(G, plans, shard(tune_range, default), sample_stride=4)
+        tuned.edge_begin, tuned.edge_end = 0, -1
+        tune_s = time.perf_counter() - t0
+
+        def trial(o):
+            ms = []
+            for r in (warm_r or timed_r)[:3]:
+                torch.cuda.synchronize()
+                t1 = time.perf_counter()
+                T.count_batch(G, plans, shard(r, o))
+                ms.append((time.perf_counter() - t1) * 1e3)
+            return min(ms)
+        d_ms, t_ms = trial(default), trial(tuned)
+        knobs = tuned if t_ms <= d_ms else default
+        launch = {"autotune": "tdfs_autotune on every 4th level-0 chunk, kept only if faster than the defaults "
+                              "over warm-up steps", "autotune_s": round(tune_s, 2),
+                  "tuned": {f: getattr(tuned, f) for f, _ in T.Options._fields_
+                            if f not in ("stream", "edge_begin", "edge_end", "edge_stride", "edge_phase")},
+                  "warmup_step_ms": {"default": d_ms, "tuned": t_ms}, "chosen": "tuned" if knobs is tuned else "default"}
+    knobs.graph_capture = 0 if args.no_capture else 1
+    launch["graph_capture"] = knobs.graph_capture
+
+    def step(rng):
+        return T.count_batch(G, plans, shard(rng, knobs))
 
     for r in warm_r:
-        step(G, r)
+        step(r)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in timed_r]
-    launch = []        # ({pattern: count}, kernel ms) per match-kernel launch
-    per_pattern = {n: 0 for n, _ in plans}
+    kernel_ms = []     # match-kernel time of each step (CUDA events inside the launch)
+    per_pattern = {n: 0 for n, _, _ in pats}
+    step_counts = []
     torch.cuda.synchronize()
     for s, r in enumerate(timed_r):
         flush.zero_()  # L2 flush between timed steps (256 MB > 126 MB L2), outside the events
         ev[s][0].record()
-        counts, kms = step(G, r)
+        counts, kms = step(r)
         ev[s][1].record()
-        launch.append(({n: c for (n, _), c in zip(plans, counts)}, kms))
-        for (n, _), c in zip(plans, counts):
+        kernel_ms.append(kms)
+        step_counts.append(counts)
+        for (n, _, _), c in zip(pats, counts):
             per_pattern[n] += c
     torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
@@ -293,268 +428,483 @@ def run_tdfs(args, rank, world, dist):
     # ---- end to end through the C ABI with host buffers ------------------
     rp = torch.from_numpy(np.ascontiguousarray(g.rowptr)).pin_memory()
     ci = torch.from_numpy(np.ascontiguousarray(g.colidx)).pin_memory()
-    lb = torch.from_numpy(np.ascontiguousarray(g.labels)).pin_memory() if labeled else None
-    h2d = rp.numel() * 8 + ci.numel() * 4 + (lb.numel() * 4 if lb is not None else 0) + sum(len(t) for _, t in pats)
+    lb = torch.from_numpy(np.ascontiguousarray(g.labels)).pin_memory() if labeled_any else None
+    h2d = rp.numel() * 8 + ci.numel() * 4 + (lb.numel() * 4 if lb is not None else 0)
     d2h = 8 * len(pats)  # one u64 count read back per pattern
+    e2e_knobs = shard((0, -1), knobs)
+    e2e_knobs.graph_capture = 0  # a fresh graph every step: nothing to replay
     e2e_s, e2e_m = 0.0, 0
     for r in timed_r:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         Gh = T.GraphPreprocessor(rowptr=rp.numpy(), colidx=ci.numpy(), labels=None if lb is None else lb.numpy(),
-                                 labeled=labeled, device=dev)
-        ps = [T.PatternPreprocessor(text=t, labeled=labeled) for _, t in pats]
-        e2e_m += sum(T.count_batch(Gh, ps, opts(r))[0])
+                                 labeled=labeled_any, device=dev)
+        ps = [T.PatternPreprocessor(text=t, labeled=lab) for _, t, lab in pats]
+        o = shard(r, e2e_knobs)
+        o.graph_capture = 0
+        e2e_m += sum(T.count_batch(Gh, ps, o)[0])
         Gh.close()
         e2e_s += time.perf_counter() - t0
     if dist:
         e2e_s, (e2e_m,) = reduce_over_ranks(dist, e2e_s, [e2e_m])
-
+    modes = len({lab for _, _, lab in pats})
     line = {
         "metric": "matches_per_s", "value": value, "unit": "matches/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32/u64",
-        "data": "synthetic (seeded generators of the benchmark config)",
-        "config": dict(desc, parallelism=f"level-0 edge chunks dealt round-robin over {world} rank(s)",
-                       l2="flushed between timed steps (256 MB write)", timed_edge_ranges=timed_r,
-                       counts=per_pattern),
+        "data": "synthetic (seeded generators of the benchmark configs)",
+        "config": dict(workload=desc, counts=per_pattern, l2="256 MB buffer written between timed steps",
+                       **({"timed_edge_ranges": timed_r} if slices > 1 else {})),
         "e2e": {"value": e2e_m / e2e_s, "unit": "matches/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "gpu_launches": 2 * args.steps,  # per step: the control reset and one batched match kernel
+                "d2h_bytes_per_step": d2h,
+                "step": "tdfs_graph_from_csr from pinned host CSR (upload + derived arrays), pattern compiles, "
+                        "tdfs_count_batch, count read-back, tdfs_graph_free"},
+        # per step and mode: the control reset and the match kernel
+        "gpu_launches": 2 * modes * args.steps,
+        "launch": launch,
+        "parallelism": f"level-0 edge chunks dealt round-robin over {world} rank(s)",
         "clocks": clk,
     }
-    return line, launch, (g, pats, labeled, timed_r)
+    return line, (g, pats, timed_r, step_counts, kernel_ms)
+
+
+def check_counts(name, got, want):
+    if got != want:
+        raise CountMismatch(f"{name}: GPU count {got} != CPU oracle {want}")
+
+
+def c2_subrecord_tdfs(args):
+    """Config 2 as stated: the 5-clique over the whole power-law graph in one
+    launch, and the house over five fixed 1/1000 slices (its whole-graph count
+    is ~1e13, stated as an estimate with its relative standard error)."""
+    import torch
+    import tdfs_b200 as T
+    g = graph_via_library(T, "cl")
+    G = T.GraphPreprocessor(csr=g)
+    E = g.nedges
+    k5 = T.PatternPreprocessor(text=clique(5))
+    house = T.PatternPreprocessor(text=HOUSE)
+    T.count(G, k5, T.default_options(edge_begin=E // 2, edge_end=E // 2 + E // 1000))  # warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r5 = T.count(G, k5)
+    e1.record()
+    torch.cuda.synchronize()
+    k5_ms = e0.elapsed_time(e1)
+    sl = [(j * E // 1000, (j + 1) * E // 1000) for j in C2_HOUSE_SLICES]
+    T.count(G, house, T.default_options(edge_begin=sl[0][0] + E // 1000, edge_end=sl[0][1] + E // 1000))
+    h_counts, h_ms = [], []
+    for b, e in sl:
+        torch.cuda.synchronize()
+        e0.record()
+        h_counts.append(T.count(G, house, T.default_options(edge_begin=b, edge_end=e)).count)
+        e1.record()
+        torch.cuda.synchronize()
+        h_ms.append(e0.elapsed_time(e1))
+    est = T.estimate(g, house, 20000, 7)
+    # oracle pins on prefixes of the measured work (the whole counts take the
+    # CPU oracle far too long): the 5-clique from the hub edges at the start
+    # of the edge array, the house from the start of its first slice, each
+    # prefix as long as the CPU oracle finishes in a few seconds
+    pins = {}
+    for pname, P, text, start in (("5-clique", k5, clique(5), 0), ("house", house, HOUSE, sl[0][0])):
+        per, _, pre = oracle_pass(g, [(pname, text, False)], [(start, sl[0][1])], budget_s=args.pin_budget)
+        b, e = pre[pname]
+        got = T.count(G, P, T.default_options(edge_begin=b, edge_end=e)).count
+        check_counts(f"c2 {pname} [{b},{e})", got, per[pname][0])
+        pins[pname] = {"edges": [b, e], "count": got}
+    return {"workload": "Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1, degree-ordered ids",
+            "5-clique": {"edges": "whole graph", "count": r5.count, "ms": k5_ms,
+                         "matches_per_s": r5.count / (k5_ms / 1e3)},
+            "house": {"slices_of_1000": list(C2_HOUSE_SLICES), "edge_ranges": sl, "counts": h_counts,
+                      "ms": h_ms, "matches_per_s": sum(h_counts) / (sum(h_ms) / 1e3),
+                      "whole_graph_estimate": {"matches": est.matches, "rse": est.matches_rse,
+                                               "probes": est.probes,
+                                               "seconds_at_measured_rate": est.matches / (sum(h_counts) /
+                                                                                          (sum(h_ms) / 1e3))}},
+            "oracle_pinned_subslices": pins}
 
 
 def run_reference(args, rank, world):
     """The reference's own CUDA kernel on the same steps: oracle/_ref/refshard_*
     drives _parallel_match (src/gpu_match.cu, compiled unchanged for sm_100a)
-    over the same edge ranges and reports its own cudaEvent kernel time."""
-    import tdfs_b200 as T
+    over the same edge ranges and reports its own cudaEvent kernel time.  The
+    graph and patterns come from tdfs_convert and the expected counts from the
+    CPU oracle's command-line tool, so this process never loads the engine."""
     if rank != 0:
         return None
+    desc, gkey, spec, slices = workload(args.workload)
     if args.workload == "c4":
         return {"impl": "reference", "unavailable": "the reference kernel writes each candidate set into a "
                 "4096-entry stack row (GRAPH_DEGREE, src/config.h:12) and this graph has vertices of degree "
                 "~400k: writes far past its stack allocation are expected, so it is not run"}
-    desc, g, pats, labeled, slices = workload(args.workload, T)
-    exe = os.path.join(ROOT, "oracle", "_ref", "refshard_lb" if labeled else "refshard_ulb")
-    if not os.path.exists(exe):
-        return {"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources)"}
-    warm_r, timed_r = step_ranges(g.nedges, slices, args.steps, args.warmup)
+    for exe in ("refshard_ulb", "refshard_lb"):
+        if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", exe)):
+            return {"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference sources)"}
     work = tempfile.mkdtemp(prefix="tdfs_ref_")
     prefix = os.path.join(work, "snap.txt")
-    g.write(prefix)
-
-    def run(text, warm, ranges):
-        # warm-up launches first, in the same process, untimed (-w)
-        p = os.path.join(work, "p.g")
-        with open(p, "w") as f:
-            f.write(text)
-        args_r = [str(x) for r in warm + ranges for x in r]
-        r = subprocess.run([exe, prefix, p, "-w", str(len(warm))] + args_r, capture_output=True, text=True,
-                           timeout=args.ref_timeout)
-        lines = [l for l in r.stdout.splitlines() if l.count("\t") == 2]
-        if r.returncode or not lines:
-            raise RuntimeError(f"reference run failed rc={r.returncode}: {r.stderr[-300:]}")
-        _, ms, c = lines[-1].split("\t")
-        return float(ms), int(c)
-
+    E = graph_via_convert(gkey, prefix)
+    pats = [(n, pattern_text(s, convert_pattern), lab) for n, s, lab in spec]
+    warm_r, timed_r = step_ranges(E, slices, args.steps, args.warmup)
     try:
-        tot_ms, tot_c, counts = 0.0, 0, {}
-        for n, t in pats:
-            ms, c = run(t, warm_r, timed_r)
-            tot_ms += ms
-            tot_c += c
-            counts[n] = c
+        res = ref_counts(prefix, work, pats, warm_r, timed_r, args.ref_timeout)
     except subprocess.TimeoutExpired:
         return {"impl": "reference", "unavailable": f"reference kernel exceeded {args.ref_timeout}s on the workload"}
     except RuntimeError as e:
         return {"impl": "reference", "unavailable": str(e)[:200]}
-    value = tot_c / (tot_ms / 1e3)
-    return {"impl": "reference", "metric": "matches_per_s", "value": value, "unit": "matches/s", "n_gpus": 1,
+    counts = {n: c for n, (ms, c) in res.items()}
+    tot_ms = sum(ms for ms, _ in res.values())
+    want = expected_counts(prefix, work, pats, timed_r, slices)
+    wrong = {n: {"reference": counts[n], "expected": want[n]} for n in counts if want.get(n) not in (None, counts[n])}
+    line = {"impl": "reference", "metric": "matches_per_s", "unit": "matches/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": tot_ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "int32/u64",
-            "data": "synthetic (seeded generators of the benchmark config)",
-            "config": dict(desc, counts=counts, timed_edge_ranges=timed_r,
-                           timing="the reference's own kernel, cudaEvent pair around each launch as cu_test.cu:81-97; "
-                                  "the warm-up launches run first in the same process, untimed",
-                           note="the reference build's counts can differ from the reference semantics on heavy "
-                                "subtrees; they are reported as printed"),
-            "cpu_baseline": {"value": value, "unit": "matches/s", "cores": 0, "kind": "reference",
-                             "sample": "the reference's own CUDA kernel on the timed steps (it has no CPU path)"},
-            "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded generators of the benchmark configs)",
+            "config": dict(workload=desc, counts=counts, l2="256 MB buffer written between timed steps",
+                           **({"timed_edge_ranges": timed_r} if slices > 1 else {})),
+            "timing": "the reference's own kernel, cudaEvent pair around each launch as cu_test.cu:81-97; one "
+                      "launch per pattern and step; warm-up launches first in the same process, untimed",
+            "count_check": "per pattern against the CPU oracle over the same steps" if slices == 1 else
+                           "against the committed counts of this workload (tests/golden/bench_counts.json)"}
+    if wrong:
+        line["unavailable"] = "reference count wrong"
+        line["wrong_counts"] = wrong
+        line["value"] = None
+    else:
+        line["value"] = sum(counts.values()) / (tot_ms / 1e3)
+    v = line["value"]
+    line["cpu_baseline"] = {"value": v, "unit": "matches/s", "cores": 0, "kind": "reference",
+                            "sample": "the reference's own CUDA kernel on the timed steps (it has no CPU path)"}
+    line["e2e"] = {"value": v, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    if args.workload == "c13" and not args.no_c2:
+        line["c2"] = c2_subrecord_reference(args, work)
+    return line
 
 
-def admit_stream(T, g, texts, max_matches, max_scanned):
-    """Indices of the queries whose estimated work (tdfs_estimate: 128 probes,
-    then 1024 for any query within 100x of the budget) fits the budget."""
-    keep = []
-    for i, t in enumerate(texts):
-        P = T.PatternPreprocessor(text=t, labeled=True)
-        r = T.estimate(g, P, 128, i)
-        if r.matches > 100 * max_matches or r.scanned > 100 * max_scanned:
-            continue
-        r = T.estimate(g, P, 1024, i)
-        if r.matches <= max_matches and r.scanned <= max_scanned:
-            keep.append(i)
-    return keep
+def ref_counts(prefix, work, pats, warm_r, timed_r, timeout):
+    """{pattern: (sum of kernel ms, count)} of refshard over the timed ranges."""
+    out = {}
+    for i, (name, text, lab) in enumerate(pats):
+        p = os.path.join(work, f"p{i}.g")
+        with open(p, "w") as f:
+            f.write(text)
+        exe = os.path.join(ROOT, "oracle", "_ref", "refshard_lb" if lab else "refshard_ulb")
+        argv = [exe, prefix, p, "-w", str(len(warm_r)), "-f"] + [str(x) for r in warm_r + timed_r for x in r]
+        r = subprocess.run(argv, capture_output=True, text=True, timeout=timeout)
+        lines = [l for l in r.stdout.splitlines() if l.count("\t") == 2]
+        if r.returncode or not lines:
+            raise RuntimeError(f"reference run failed rc={r.returncode}: {r.stderr[-300:]}")
+        _, ms, c = lines[-1].split("\t")
+        out[name] = (float(ms), int(c))
+    return out
+
+
+def golden_bench_counts():
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "bench_counts.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def expected_counts(prefix, work, pats, timed_r, slices):
+    """The counts the reference semantics give over the timed steps: the CPU
+    oracle's command-line tool on whole-graph steps, else the committed counts
+    of the workload's slices (None where unknown)."""
+    want = {}
+    if slices == 1:
+        for i, (name, _, lab) in enumerate(pats):
+            p = os.path.join(work, f"p{i}.g")
+            argv = [ORACLE_CLI] + (["--labeled"] if lab else []) + [prefix, p]
+            line = subprocess.run(argv, capture_output=True, text=True, check=True).stdout.splitlines()[-1]
+            want[name] = int(line.split("\t")[2]) * len(timed_r)
+        return want
+    gold = golden_bench_counts()
+    for name, _, _ in pats:
+        rec = gold.get("c2_slices", {}).get(name, {})
+        vals = [rec.get(f"{b},{e}") for b, e in timed_r]
+        want[name] = None if None in vals else sum(vals)
+    return want
+
+
+def c2_subrecord_reference(args, work):
+    """The c2 sub-record on the reference build: the 5-clique over the whole
+    graph and the house over the same five slices, compared with the
+    committed counts of this engine (tests/golden/bench_counts.json, pinned to
+    the CPU oracle on sub-slices by the GPU tests)."""
+    prefix = os.path.join(work, "cl")
+    E = graph_via_convert("cl", prefix)
+    sl = [(j * E // 1000, (j + 1) * E // 1000) for j in C2_HOUSE_SLICES]
+    gold = golden_bench_counts().get("c2", {})
+    rec = {"workload": "Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1, degree-ordered ids"}
+    try:
+        k5 = ref_counts(prefix, work, [("5-clique", clique(5), False)], [(E // 2, E // 2 + E // 1000)], [(0, E)],
+                        args.ref_timeout)["5-clique"]
+        hs = [ref_counts(prefix, work, [("house", HOUSE, False)], [], [r], args.ref_timeout)["house"] for r in sl]
+    except (subprocess.TimeoutExpired, RuntimeError) as e:
+        return {"unavailable": f"reference run failed: {str(e)[:160]}"}
+    rec["5-clique"] = {"edges": "whole graph", "count": k5[1], "ms": k5[0], "expected": gold.get("5-clique")}
+    rec["house"] = {"edge_ranges": sl, "counts": [c for _, c in hs], "ms": [m for m, _ in hs],
+                    "expected": gold.get("house")}
+    ok = gold and k5[1] == gold.get("5-clique") and [c for _, c in hs] == gold.get("house")
+    if not ok:
+        rec["unavailable"] = "reference count wrong" if gold else "no committed counts to check against"
+    else:
+        rec["matches_per_s"] = (k5[1] + sum(c for _, c in hs)) / ((k5[0] + sum(m for m, _ in hs)) / 1e3)
+    return rec
+
+
+# ---- served stream (c5) -------------------------------------------------------
+
+def c5_queries(gen, n):
+    """The config-5 stream: n random connected labeled queries of 3-7 vertices,
+    edge density U[0.3, 0.8], labels U[0,4), seed 5."""
+    import random
+    rng = random.Random(5)
+    return [gen(rng.randint(3, 7), rng.uniform(0.3, 0.8), 4, 5 * 1_000_003 + i) for i in range(n)]
 
 
 def run_serve(args):
-    """The served stream (c5): random labeled 3-7 vertex queries (density
-    U[0.3, 0.8], labels U[0,4), seed 5) against the power-law graph of c2 with
-    labels U[0,4), seed 2.  Most such queries on this graph have
-    1e9 to 1e16 matches (sparse 7-vertex patterns around 20k-degree hubs), far
-    beyond any DFS in a benchmark; the stream is admitted by estimated work
-    (tdfs_estimate) and the admitted queries are run four ways: sequential
-    plain launches, batched launches (one slot per query), the continuous-
-    batching server with every query submitted at once (capacity), and the
-    server under Poisson arrivals at half that capacity (p50/p99 latency).
-    Every count must equal its plain count."""
+    """The served stream (config 5): every one of the --queries random labeled
+    queries against the labeled power-law graph (config 2's graph with labels
+    U[0,4), seed 2).  Most such queries have 1e9 to 1e16 matches on this graph
+    (sparse 7-vertex patterns around 20k-degree hubs), so every query carries
+    a device-side work budget (--budget units: one per DFS node claimed and per
+    32-wide scan step); a query that runs out is abandoned on the device and
+    answered with TDFS_ERR_TIMEOUT, the others with their exact count.
+
+    Queries are admitted by their memory charge (slot record + one CTA's DFS
+    stack + split units) into one persistent launch that stays up across
+    arrival gaps, with launch knobs from tdfs_autotune on a sample of the
+    stream.  Four ways over the same queries and budget: sequential plain
+    launches (a sample of --plain-sample queries), one batched launch, the
+    server with every query submitted at once (capacity), and the server under
+    Poisson arrivals at --rate (default half the capacity) for p50/p99.  Every
+    count that completes in two modes must be identical."""
     import random
-    import threading
     import torch
     import tdfs_b200 as T
     torch.cuda.set_device(0)
     g = T.gen_chung_lu(1_100_000, 3_000_000, 2.1, 30_000, 1).set_labels(4, 2)
     G = T.GraphPreprocessor(csr=g, labeled=True)
-    rng = random.Random(5)
-    texts = [T.gen_pattern(rng.randint(3, 7), rng.uniform(0.3, 0.8), 4, 5 * 1_000_003 + i) for i in range(args.queries)]
+    texts = c5_queries(T.gen_pattern, args.queries)
+    qs = [T.PatternPreprocessor(text=t, labeled=True) for t in texts]
+    B = int(args.budget)
+    base = T.default_options(work_budget=B)
+    # launch knobs: the autotuner on a sample of the stream
     t0 = time.perf_counter()
-    admitted = admit_stream(T, g, texts, args.max_matches, args.max_scanned)
-    t_est = time.perf_counter() - t0
-    qs = [T.PatternPreprocessor(text=texts[i], labeled=True) for i in admitted]
-    for q in qs[:8]:
-        T.count(G, q)  # warm-up
-    torch.cuda.synchronize()
+    sample = qs[:: max(1, len(qs) // 64)][:64]
+    tuned, _ = T.autotune(G, sample, base, sample_stride=4)
+    tuned.edge_begin, tuned.edge_end, tuned.edge_stride, tuned.edge_phase = 0, -1, 1, 0
+    tuned.work_budget = B
+    tune_s = time.perf_counter() - t0
+    T.count_batch_status(G, qs[:16], tuned)  # warm-up
+
+    def tally(res):
+        return {"completed": sum(r is not None for r in res), "budget_exceeded": sum(r is None for r in res)}
+
+    # plain: one launch per query, on an evenly spread sample
+    pick = list(range(0, len(qs), max(1, len(qs) // args.plain_sample)))[:args.plain_sample]
     t0 = time.perf_counter()
-    plain = [T.count(G, q).count for q in qs]
-    t_seq = time.perf_counter() - t0
-    seq_qps = len(qs) / t_seq
-    # batched: one persistent launch per 4096 queries
+    plain = {}
+    for i in pick:
+        c, st, _ = T.count_batch_status(G, [qs[i]], tuned)
+        plain[i] = c[0] if st[0] == 0 else None
+    t_plain = time.perf_counter() - t0
+    # batched: every query in one persistent launch
     t0 = time.perf_counter()
-    batched = []
-    for b in range(0, len(qs), 4096):
-        batched += T.count_batch(G, qs[b:b + 4096])[0]
+    c, st, _ = T.count_batch_status(G, qs, tuned)
     t_batch = time.perf_counter() - t0
-    # served, every query submitted at once
-    srv = T.Server(G, labeled=True, max_inflight=args.inflight)
-    t0 = time.perf_counter()
-    tickets = [srv.submit(q) for q in qs]
-    served = [srv.wait(tk)[0] for tk in tickets]
-    t_srv = time.perf_counter() - t0
-    srv.close()
+    batched = [ci if si == 0 else None for ci, si in zip(c, st)]
+
+    def serve(rate):
+        srv = T.Server(G, labeled=True, max_inflight=args.inflight, idle_exit_ms=5000,
+                       **{f: getattr(tuned, f) for f, _ in T.Options._fields_
+                          if f not in ("stream", "edge_begin", "edge_end", "edge_stride", "edge_phase")})
+        tickets = [None] * len(qs)
+        arr = random.Random(55)
+
+        def producer():
+            t = time.perf_counter()
+            for i, q in enumerate(qs):
+                if rate > 0:
+                    t += arr.expovariate(rate)
+                    d = t - time.perf_counter()
+                    if d > 0:
+                        time.sleep(d)
+                tickets[i] = srv.submit(q)
+
+        th = threading.Thread(target=producer)
+        t1 = time.perf_counter()
+        th.start()
+        th.join()
+        out = []
+        for tk in tickets:
+            try:
+                out.append(srv.wait(tk)[0])
+            except T.TdfsError as e:
+                if e.code != 6:
+                    raise
+                out.append(None)
+        dt = time.perf_counter() - t1
+        st = srv.stats()
+        srv.close()
+        return out, dt, st
+
+    served, t_srv, st_cap = serve(0.0)
     cap_qps = len(qs) / t_srv
-    # served under Poisson arrivals
     rate = args.rate if args.rate > 0 else 0.5 * cap_qps
-    srv = T.Server(G, labeled=True, max_inflight=args.inflight)
-    tickets = [None] * len(qs)
-    arr = random.Random(55)
+    poisson, t_poisson, st = serve(rate)
 
-    def producer():
-        t = time.perf_counter()
-        for i, q in enumerate(qs):
-            t += arr.expovariate(rate)
-            d = t - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            tickets[i] = srv.submit(q)
-
-    th = threading.Thread(target=producer)
-    t1 = time.perf_counter()
-    th.start()
-    th.join()
-    poisson = [srv.wait(tk)[0] for tk in tickets]
-    t_poisson = time.perf_counter() - t1
-    st = srv.stats()
-    srv.close()
-    ok = batched == plain and served == plain and poisson == plain
+    def agree(a, b, idx):
+        both = [i for i in idx if a[i] is not None and b[i] is not None]
+        return {"both_completed": len(both), "identical": all(a[i] == b[i] for i in both),
+                "flipped": sum((a[i] is None) != (b[i] is None) for i in idx)}
+    allidx = range(len(qs))
+    plain_l = [plain.get(i) for i in allidx]
+    checks = {"plain_vs_batched": agree(plain_l, batched, pick), "batched_vs_served": agree(batched, served, allidx),
+              "batched_vs_poisson": agree(batched, poisson, allidx)}
+    ok = all(v["identical"] for v in checks.values())
     return {"metric": "served_queries_per_s", "value": cap_qps, "unit": "queries/s", "n_gpus": 1,
             "steps": 1, "warmup": 1, "ms_per_step": t_srv * 1e3, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "int32/u64", "data": "synthetic (seeded generators of the benchmark config)",
             "config": {"workload": f"{args.queries} random labeled queries (3-7 vertices, density U[0.3,0.8], labels "
                                    "U[0,4), seed 5) on Chung-Lu n=1.1M m=3.0M gamma=2.1 cap=30k seed 1 with labels "
-                                   f"U[0,4) seed 2; {len(qs)} admitted by estimated work (<= {args.max_matches:.0e} "
-                                   f"matches and <= {args.max_scanned:.0e} scanned adjacency entries)",
-                       "queries_drawn": args.queries, "queries_admitted": len(qs), "estimate_s": t_est,
-                       "max_inflight": args.inflight},
-            "sequential_plain_queries_per_s": seq_qps, "batched_queries_per_s": len(qs) / t_batch,
-            "served_saturated_queries_per_s": cap_qps,
-            "poisson": {"rate_per_s": rate, "queries_per_s": len(qs) / t_poisson, "p50_ms": st["p50_us"] / 1e3,
-                        "p99_ms": st["p99_us"] / 1e3},
-            "counts_identical_to_plain": ok, "matches_total": sum(plain)}
+                                   f"U[0,4) seed 2; every query served, each with a device work budget of {B} units",
+                       "work_budget": B, "max_inflight": args.inflight},
+            "launch": {"autotune_s": round(tune_s, 2),
+                       "tuned": {f: getattr(tuned, f) for f, _ in T.Options._fields_
+                                 if f not in ("stream", "edge_begin", "edge_end", "edge_stride", "edge_phase")}},
+            "served_capacity": dict(tally(served), queries_per_s=cap_qps, p50_ms=st_cap["p50_us"] / 1e3,
+                                    p99_ms=st_cap["p99_us"] / 1e3, launches="one persistent kernel"),
+            "poisson": dict(tally(poisson), rate_per_s=rate, queries_per_s=len(qs) / t_poisson,
+                            p50_ms=st["p50_us"] / 1e3, p99_ms=st["p99_us"] / 1e3, max_ms=st["max_us"] / 1e3),
+            "batched": dict(tally(batched), queries_per_s=len(qs) / t_batch),
+            "sequential_plain": dict(tally([plain[i] for i in pick]), queries=len(pick),
+                                     queries_per_s=len(pick) / t_plain),
+            "counts_identical": ok, "checks": checks,
+            "matches_total_completed": sum(x for x in batched if x is not None)}
+
+
+def finish_line(args, line, aux):
+    """CPU oracle: every count of the timed steps (whole-graph steps) or of a
+    bounded prefix (slices), the CPU baseline on the same work, and the
+    roofline from exact model bytes."""
+    import tdfs_b200 as T
+    g, pats, timed_r, step_counts, kernel_ms = aux
+    peak, kind = measured_hbm_peak()
+    whole = len(set(timed_r)) == 1 and timed_r[0] == (0, g.nedges)
+    if whole:
+        # the oracle over one whole step gives every count and the exact bytes;
+        # it is repeated for the CPU baseline until the budget is spent
+        per, spent, _ = oracle_pass(g, pats, [timed_r[0]])
+        for s, cs in enumerate(step_counts):
+            for (n, _, _), c in zip(pats, cs):
+                check_counts(f"{n} step {s}", c, per[n][0])
+        passes, t_cpu = 1, spent
+        while t_cpu < args.cpu_budget:
+            t_cpu += oracle_pass(g, pats, [timed_r[0]])[1]
+            passes += 1
+        step_matches = sum(c for c, _ in per.values())
+        line["cpu_baseline"] = {"value": passes * step_matches / t_cpu, "unit": "matches/s",
+                                "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": f"the CPU oracle (all host threads) over {passes} whole step(s)",
+                                "seconds": round(t_cpu, 2)}
+        bytes_launch = sum(b for _, b in per.values())
+        line["count_check"] = "every timed step's count per pattern equals the CPU oracle's"
+        model = "exact, from the CPU oracle over the same step"
+    else:
+        per, spent, prefixes = oracle_pass(g, pats, [timed_r[0]], budget_s=args.cpu_budget)
+        G = T.GraphPreprocessor(csr=g, labeled=any(lab for _, _, lab in pats))
+        for n, t, lab in pats:
+            b, e = prefixes[n]
+            got = T.count(G, T.PatternPreprocessor(text=t, labeled=lab), T.default_options(edge_begin=b,
+                                                                                         edge_end=e)).count
+            check_counts(f"{n} edges [{b},{e})", got, per[n][0])
+        line["cpu_baseline"] = {"value": sum(c for c, _ in per.values()) / spent, "unit": "matches/s",
+                                "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": "the CPU oracle (all host threads) on prefixes of the first timed step (" +
+                                          "; ".join(f"{n}: edges [{b}, {e})" for n, (b, e) in prefixes.items()) + ")",
+                                "seconds": round(spent, 2)}
+        # model bytes per match from the prefix, times each pattern's matches
+        bytes_launch = statistics.mean(
+            sum(per[n][1] / per[n][0] * c for (n, _, _), c in zip(pats, cs) if per[n][0] > 0) for cs in step_counts)
+        line["count_check"] = "the GPU count over each pattern's CPU prefix equals the CPU oracle's"
+        model = "per-match bytes of the CPU prefix times the launch's matches (an extrapolation)"
+    mean_s = statistics.mean(kernel_ms) / 1e3
+    achieved = bytes_launch / mean_s / 1e9
+    prof = measured_profile(args.workload)
+    line["roofline"] = {
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+        "peak_kind": kind, "traffic": prof["dram_bytes_per_launch"] if prof else None,
+        "algorithmic_bytes_per_launch": bytes_launch, "mean_kernel_ms": mean_s * 1e3,
+        "bytes_model": "reference-plan merge model: 4 B x (|set1|+|set2|) per set operation, 16 B per adjacency "
+                       "lookup, 8 B per level-0 edge; " + model,
+        "note": "the graph is L2-resident: the model bytes are served by shared memory, L1 and L2, so frac is "
+                "not a DRAM utilisation; the binding limits are in `limits`"}
+    if prof:
+        line["roofline"]["dram_frac"] = prof["dram_bytes_per_launch"] / mean_s / 1e9 / peak
+        line["limits"] = {k: prof[k] for k in ("issue_active_pct", "warps_active_pct", "l2_bytes_per_launch",
+                                               "l2_throughput_pct", "long_scoreboard_per_issue") if k in prof}
+        line["limits"]["source"] = prof.get("command")
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="c13", choices=["c13", "c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--no-c2", action="store_true", help="c13: skip the config-2 sub-record")
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-capture", action="store_true")
     ap.add_argument("--queries", type=int, default=10000, help="c5: queries drawn for the served stream")
-    ap.add_argument("--max-matches", type=float, default=2e9, help="c5: admit queries estimated below this count")
-    ap.add_argument("--max-scanned", type=float, default=2e10,
-                    help="c5: admit queries estimated to scan fewer adjacency entries")
+    ap.add_argument("--budget", type=float, default=2e6, help="c5: device work budget per query (units)")
+    ap.add_argument("--plain-sample", type=int, default=500, help="c5: queries also run as single plain launches")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: Poisson arrival rate (0 = half the served capacity)")
     ap.add_argument("--inflight", type=int, default=256, help="c5: server in-flight limit")
     ap.add_argument("--impl", default="tdfs", choices=["tdfs", "reference"])
-    ap.add_argument("--cpu-budget", type=float, default=12.0, help="seconds of CPU-oracle work for cpu_baseline")
+    ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU-oracle work for cpu_baseline")
     ap.add_argument("--ref-timeout", type=int, default=600)
+    ap.add_argument("--pin-budget", type=float, default=4.0,
+                    help="c2 sub-record: seconds of CPU-oracle work per pattern for its count pins")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     dist = None
+    if args.impl == "reference":
+        # rank 0 alone runs the reference; the other ranks exit without work
+        if rank == 0:
+            print(json.dumps(run_reference(args, rank, world)), flush=True)
+        return
     if world > 1:
         import datetime
+        import torch
         import torch.distributed as dist
-        if args.impl == "tdfs":
-            import torch
-            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        dist.init_process_group("nccl" if args.impl == "tdfs" else "gloo", timeout=datetime.timedelta(seconds=900))
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
     if args.workload == "c5":
         if rank == 0:
             print(json.dumps(run_serve(args)), flush=True)
         return
-    if args.impl == "reference":
-        line = run_reference(args, rank, world)
+    try:
+        line, aux = run_tdfs(args, rank, world, dist)
         if rank == 0:
+            if world == 1:
+                finish_line(args, line, aux)
+            else:
+                line["cpu_baseline"] = None
+            if args.workload == "c13" and not args.no_c2 and world == 1:
+                line["c2"] = c2_subrecord_tdfs(args)
             print(json.dumps(line), flush=True)
+    except CountMismatch as e:
+        print(json.dumps({"error": "count mismatch", "detail": str(e)}), flush=True)
+        sys.exit(3)
+    finally:
         if dist:
             dist.barrier()
             dist.destroy_process_group()
-        return
-    line, launch, (g, pats, labeled, timed_r) = run_tdfs(args, rank, world, dist)
-    if rank == 0:
-        peak, kind = measured_hbm_peak()
-        per = {}
-        if world == 1:
-            cb, per = cpu_baseline(g, pats, labeled, timed_r[0], args.cpu_budget)
-            line["cpu_baseline"] = cb
-        else:
-            line["cpu_baseline"] = None
-        # roofline of the match kernel: merge-model bytes per match (oracle
-        # sample, per pattern) x each pattern's matches in the launch / mean
-        # launch time
-        usable = [(cs, ms) for cs, ms in launch if ms > 0]
-        if usable and any(n in per and per[n][1] > 0 for n in usable[0][0]):
-            bytes_launch = [sum(per[n][0] / per[n][1] * c for n, c in cs.items() if n in per and per[n][1] > 0)
-                            for cs, _ in usable]
-            mean_b = statistics.mean(bytes_launch)
-            mean_s = statistics.mean(ms for _, ms in usable) / 1e3
-            achieved = mean_b / mean_s / 1e9
-            line["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                                "frac": achieved / peak, "peak_kind": kind,
-                                "traffic": measured_traffic(args.workload),
-                                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per timed "
-                                                  "launch, profiles/match_kernel_traffic.json",
-                                "bytes_per_launch": mean_b, "mean_launch_ms": mean_s * 1e3,
-                                "bytes_model": "reference-plan merge model (4 B x (|set1|+|set2|) per set op, "
-                                               "16 B per list lookup, 8 B per level-0 edge); bytes per match "
-                                               "from the CPU-oracle sample, per pattern"}
-        print(json.dumps(line), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -64,9 +64,16 @@ typedef struct {
   int steal_first;      /* an idle warp first takes a level with >= steal_first items from a warp
                            of its CTA, then a unit of the split ring, and only then a level
                            with >= steal_min items (0 auto = 8) */
-  int lane_list;        /* last level with a staged fixed set: a parent whose adjacency list is
-                           at most this long is counted by one lane, 32 parents at once
-                           (0 auto = 8, -1 off: one parent per warp pass) */
+  int lane_list;        /* last level with a staged fixed set: up to 32 siblings are counted in
+                           one flattened warp pass over their adjacency lists laid end to end;
+                           lists longer than max(lane_list, 4 x the fixed set) are counted one by
+                           one (0 auto = 32, -1 off: one warp pass per sibling) */
+  int64_t work_budget;  /* work units each pattern (or served query) may spend, 0 = unlimited: one
+                           unit per DFS node claimed and per 32-wide adjacency scan step.  A pattern
+                           that runs out is abandoned on the device and reported with
+                           TDFS_ERR_TIMEOUT; the others complete normally */
+  int wait_limit_ms;    /* bound on a warp's idle wait for work before the launch reports
+                           TDFS_ERR_TIMEOUT (0 auto = 30000) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);
@@ -110,6 +117,20 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
  * All plans run in one persistent launch; counts[i] belongs to plans[i]. */
 int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
                      const tdfs_options *opt, uint64_t *counts, float *kernel_ms);
+/* Same, with a status per plan: status[i] = TDFS_OK, or TDFS_ERR_TIMEOUT when
+ * plan i ran out of opt->work_budget (counts[i] is then 0).  Returns TDFS_OK
+ * when the launch itself succeeded.  tdfs_count_batch returns TDFS_ERR_TIMEOUT
+ * when any plan ran out. */
+int tdfs_count_batch_status(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
+                            const tdfs_options *opt, uint64_t *counts, int *status, float *kernel_ms);
+
+/* ---- bounded device waits, shown to run out (no reference counterpart) ----
+ * Launches the match kernel over a slot that can never complete (admitted,
+ * no level-0 tickets, no work held), so every warp waits for work until its
+ * wait_limit_ms bound runs out, then the kernel returns.  Returns the status
+ * the launch reports -- TDFS_ERR_TIMEOUT when the bound works -- and the
+ * kernel's duration in *kernel_ms.  The context stays usable afterwards. */
+int tdfs_selftest_wait_limit(tdfs_graph *g, int wait_limit_ms, float *kernel_ms);
 
 /* ---- autotuner (no reference counterpart; the reference's shape is fixed at
  *      compile time, src/config.h:15-27) ---------------------------------------
@@ -132,7 +153,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
 typedef struct tdfs_server tdfs_server;
 
 typedef struct {
-  int max_inflight;     /* queries on the device at once (<= 2048) */
+  int max_inflight;     /* queries on the device at once (<= 8192) */
   int max_k;            /* largest pattern the stack layout holds (3..7) */
   int labeled;          /* lb (1) or ulb (0) queries */
   int idle_exit_ms;     /* the kernel retires after this long idle; relaunched on demand */
@@ -141,11 +162,12 @@ typedef struct {
 } tdfs_server_options;
 
 typedef struct {
-  uint64_t completed;
+  uint64_t completed;   /* finished queries, those that ran out of their budget included */
   uint64_t pending;     /* submitted, not yet admitted */
   uint64_t inflight;    /* admitted, not yet complete */
   double p50_us, p99_us, max_us;  /* submit -> completion seen on the host */
   double queries_per_s; /* completed / (last completion - first submit) */
+  uint64_t aborted;     /* queries that ran out of the work budget (launch.work_budget) */
 } tdfs_serve_stats;
 
 void tdfs_server_options_default(tdfs_server_options *opt);
@@ -163,7 +185,7 @@ int tdfs_server_destroy(tdfs_server *s); /* drains admitted queries, stops the k
  * int32, needed for a labeled pattern) and every working buffer lives in one fixed 48 MiB array inside the
  * library's device image, held on each GPU that uses the library until the
  * process exits.  Graphs whose derived arrays do not fit in it are rejected
- * with TDFS_ERR_CAPACITY (about 4*E + 5*n bytes, up to ~35 MiB, must fit).
+ * with TDFS_ERR_CAPACITY (about 4*E + 5*n bytes, up to ~30 MiB, must fit).
  * d_colidx must be 16-byte aligned (TDFS_ERR_ARG otherwise): the kernel reads
  * adjacency windows with 16-byte loads.  When E is not a multiple of 4 those
  * windows are turned off, so nothing past colidx[E-1] is read.  The first

@@ -3,11 +3,13 @@
 // level-0 edge ranges, so the reference can be timed on the same bounded
 // slices of a workload as this repository's engine.
 //
-//   refshard_{ulb,lb} <graph prefix> <pattern.g> [-w K] <begin> <end> [<begin> <end> ...]
+//   refshard_{ulb,lb} <graph prefix> <pattern.g> [-w K] [-f] <begin> <end> [<begin> <end> ...]
 //
 // With -w K the first K ranges are warm-up launches in the same process
 // (module loading and first-touch costs land there) and are neither timed
-// nor counted.
+// nor counted.  With -f a 256 MB buffer is written before every launch,
+// outside the timed event pair, so each timed launch starts with an L2
+// that holds none of the graph (B200's L2 is 126 MB).
 //
 // Set-up follows the reference driver (cu_test.cu:14-78): the reference's
 // GraphPreprocessor / PatternPreprocessor / build_src_vtx / to_gpu, per-warp
@@ -43,12 +45,20 @@ static const int kQueueCapTriples = 1000000;  // TIMEOUT_QUEUE_CAP, cu_test.cu:8
 
 int main(int argc, char **argv) {
   int first = 3, warm = 0;
-  if (argc > 4 && std::strcmp(argv[3], "-w") == 0) {
-    warm = std::atoi(argv[4]);
-    first = 5;
+  bool flush = false;
+  while (first < argc && argv[first][0] == '-') {
+    if (std::strcmp(argv[first], "-w") == 0 && first + 1 < argc) {
+      warm = std::atoi(argv[first + 1]);
+      first += 2;
+    } else if (std::strcmp(argv[first], "-f") == 0) {
+      flush = true;
+      first += 1;
+    } else {
+      break;
+    }
   }
   if (argc < first + 2 || (argc - first) % 2 || warm < 0) {
-    fprintf(stderr, "usage: %s <prefix> <pattern.g> [-w K] <begin> <end> [<begin> <end> ...]\n", argv[0]);
+    fprintf(stderr, "usage: %s <prefix> <pattern.g> [-w K] [-f] <begin> <end> [<begin> <end> ...]\n", argv[0]);
     return 2;
   }
   CK(cudaSetDevice(0));
@@ -94,6 +104,9 @@ int main(int argc, char **argv) {
   tq->size_ = kQueueCapTriples * (STOP_LEVEL + 1);
   tq->resetQueue();
 
+  void *l2flush = nullptr;
+  const size_t kFlushBytes = size_t(256) << 20;
+  if (flush) CK(cudaMalloc(&l2flush, kFlushBytes));
   cudaEvent_t start, stop;
   CK(cudaEventCreate(&start));
   CK(cudaEventCreate(&stop));
@@ -110,6 +123,7 @@ int main(int argc, char **argv) {
     const graph_edge_t ne = end;
     CK(cudaMemcpy((char *)gpu_graph + offsetof(Graph, nedges), &ne, sizeof ne, cudaMemcpyHostToDevice));
     CK(cudaMemset(gpu_res, 0, sizeof(size_t) * NWARPS_TOTAL));
+    if (l2flush) CK(cudaMemset(l2flush, r & 0xff, kFlushBytes));
     CK(cudaDeviceSynchronize());
     CK(cudaEventRecord(start));
     _parallel_match<<<GRID_DIM, BLOCK_DIM>>>(gpu_graph, gpu_pattern, gpu_callstack, gpu_queue, gpu_res, idle_warps,

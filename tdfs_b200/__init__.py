@@ -34,7 +34,7 @@ EXPORTS = [
     "tdfs_last_error", "tdfs_version", "tdfs_options_default",
     "tdfs_graph_open", "tdfs_graph_from_csr", "tdfs_graph_info", "tdfs_graph_free",
     "tdfs_plan_compile", "tdfs_plan_from_text", "tdfs_plan_dump", "tdfs_plan_info", "tdfs_plan_free",
-    "tdfs_count", "tdfs_count_batch",
+    "tdfs_count", "tdfs_count_batch", "tdfs_count_batch_status", "tdfs_selftest_wait_limit",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
     "tdfs_csr_from_arrays", "tdfs_csr_relabel", "tdfs_csr_halve",
     "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern", "tdfs_estimate",
@@ -70,6 +70,8 @@ class Options(C.Structure):
         ("split_after_us", C.c_int),
         ("steal_first", C.c_int),
         ("lane_list", C.c_int),
+        ("work_budget", C.c_int64),
+        ("wait_limit_ms", C.c_int),
     ]
 
 
@@ -95,6 +97,7 @@ class ServeStats(C.Structure):
         ("p99_us", C.c_double),
         ("max_us", C.c_double),
         ("queries_per_s", C.c_double),
+        ("aborted", C.c_uint64),
     ]
 
 
@@ -127,6 +130,9 @@ def lib() -> C.CDLL:
     L.tdfs_count.argtypes = [vp, vp, C.POINTER(Options), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
     L.tdfs_count_batch.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_float)]
+    L.tdfs_count_batch_status.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), C.POINTER(C.c_uint64),
+                                          C.POINTER(ci), C.POINTER(C.c_float)]
+    L.tdfs_selftest_wait_limit.argtypes = [vp, ci, C.POINTER(C.c_float)]
     L.tdfs_csr_read.argtypes = [C.c_char_p, ci, pp]
     L.tdfs_csr_view.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), pp, pp, pp, C.POINTER(i32)]
     L.tdfs_csr_write.argtypes = [vp, C.c_char_p]
@@ -365,6 +371,28 @@ def count_batch(graph: GraphPreprocessor, patterns, options: Options | None = No
     _check(lib().tdfs_count_batch(graph._h, arr, len(patterns), None if options is None else C.byref(options),
                                   out, C.byref(ms)))
     return list(out), ms.value
+
+
+def count_batch_status(graph: GraphPreprocessor, patterns, options: Options | None = None):
+    """Counts and per-pattern status (0, or the TDFS_ERR_TIMEOUT code when a
+    pattern ran out of options.work_budget); returns (counts, status, kernel ms)."""
+    n = len(patterns)
+    arr = (C.c_void_p * n)(*[p._h.value for p in patterns])
+    out = (C.c_uint64 * n)()
+    st = (C.c_int * n)()
+    ms = C.c_float()
+    _check(lib().tdfs_count_batch_status(graph._h, arr, n, None if options is None else C.byref(options), out, st,
+                                         C.byref(ms)))
+    return list(out), list(st), ms.value
+
+
+def selftest_wait_limit(graph: GraphPreprocessor, wait_limit_ms: int):
+    """Run the match kernel over a slot that can never complete; returns
+    (status code the launch reported, kernel ms).  TDFS_ERR_TIMEOUT (6) means
+    every warp's bounded wait ran out as designed."""
+    ms = C.c_float()
+    rc = lib().tdfs_selftest_wait_limit(graph._h, wait_limit_ms, C.byref(ms))
+    return rc, ms.value
 
 
 EDGE_CHUNK = 32  # directed edges per level-0 ticket (kEdgeChunk in match.cuh)

@@ -6,8 +6,10 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -68,10 +70,13 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.split_after_ns = o.split_after_us > 0 ? o.split_after_us * 1000 : (o.split_after_us < 0 ? 0 : 150000);
   c.warp_bytes = (int)((warp_smem_bytes(kmax, cap, window, c.fixed != 0) + 15) & ~(size_t)15);
   c.steal = o.steal < 0 ? 1 : (o.steal ? 1 : 0);
-  c.idle_ms = 30000;
+  if (o.wait_limit_ms < 0) return fail(TDFS_ERR_ARG, "wait_limit_ms must be >= 0");
+  if (o.work_budget < 0) return fail(TDFS_ERR_ARG, "work_budget must be >= 0");
+  c.idle_ms = o.wait_limit_ms > 0 ? o.wait_limit_ms : 30000;
+  c.budgeted = o.work_budget > 0 ? 1 : 0;
   c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
   c.steal_first = o.steal_first > 0 ? o.steal_first : 8;
-  c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 8);
+  c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 32);
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
   if (c.steal_first < 2 || c.steal_first > 4096) return fail(TDFS_ERR_ARG, "steal_first must lie in [2, 4096]");
@@ -82,10 +87,27 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   if (smem > (size_t)prop.sharedMemPerBlockOptin)
     return fail(TDFS_ERR_CAPACITY, "per-CTA shared memory %zu exceeds %zu; lower chunk_cap or warps_per_block",
                 smem, (size_t)prop.sharedMemPerBlockOptin);
-  const int fit = resident_blocks_per_sm(labeled, s.warps_per_block, smem, false);
-  const int fit_wide = resident_blocks_per_sm(labeled, s.warps_per_block, smem, true);
-  if (fit < 0 || fit_wide < 0)
-    return fail(TDFS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+  // occupancy of both register budgets, cached per (device, mode, CTA shape):
+  // the queries set a kernel attribute and cost tens of microseconds, which
+  // a small launch would otherwise pay on every call
+  int fit = -1, fit_wide = -1;
+  {
+    static std::map<std::tuple<int, bool, int, size_t>, std::pair<int, int>> occ;
+    static std::mutex occ_mu;
+    const auto key = std::make_tuple(g->device, labeled, s.warps_per_block, smem);
+    std::lock_guard<std::mutex> lk(occ_mu);
+    auto it = occ.find(key);
+    if (it == occ.end()) {
+      fit = resident_blocks_per_sm(labeled, s.warps_per_block, smem, false);
+      fit_wide = resident_blocks_per_sm(labeled, s.warps_per_block, smem, true);
+      if (fit < 0 || fit_wide < 0)
+        return fail(TDFS_ERR_CUDA, "occupancy query failed: %s", cudaGetErrorString(cudaGetLastError()));
+      occ[key] = {fit, fit_wide};
+    } else {
+      fit = it->second.first;
+      fit_wide = it->second.second;
+    }
+  }
   if (fit == 0) return fail(TDFS_ERR_CAPACITY, "the match kernel does not fit on an SM with this shape");
   // a persistent grid: every CTA resident at once (idle warps wait on busy ones);
   // the 80-register build whenever it holds as many CTAs per SM
@@ -116,6 +138,7 @@ struct GraphEntry {
   int blocks, warps;
   KernelCfg cfg;
   cudaGraphExec_t exec;
+  cudaEvent_t k0, k1;  // recorded inside the graph around the match kernel
 };
 
 }  // namespace
@@ -123,7 +146,11 @@ struct GraphEntry {
 void release_graphs(tdfs_graph *g) {
   if (!g->graphs) return;
   auto *v = static_cast<std::vector<GraphEntry> *>(g->graphs);
-  for (auto &c : *v) cudaGraphExecDestroy(c.exec);
+  for (auto &c : *v) {
+    cudaGraphExecDestroy(c.exec);
+    cudaEventDestroy(c.k0);
+    cudaEventDestroy(c.k1);
+  }
   delete v;
   g->graphs = nullptr;
 }
@@ -135,7 +162,8 @@ std::vector<GraphEntry> &graph_cache(tdfs_graph *g) {
   return *static_cast<std::vector<GraphEntry> *>(g->graphs);
 }
 
-int enqueue_launch(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, cudaStream_t st) {
+int enqueue_launch(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, cudaStream_t st, cudaEvent_t k0,
+                   cudaEvent_t k1) {
   SlotTable *h = g->htab, *d = g->tab;
   cudaError_t e = cudaMemcpyAsync(&d->ctl, &h->ctl, sizeof h->ctl, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d->hot, h->hot, sizeof(SlotHot) * n, cudaMemcpyHostToDevice, st);
@@ -143,74 +171,88 @@ int enqueue_launch(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, cud
   if (e == cudaSuccess) e = cudaMemcpyAsync(d->plan, h->plan, sizeof(DevPlan) * n, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_err(e, "slot table upload");
   init_launch(g->ctl, queue_hdr(g), st);
+  e = cudaEventRecord(k0, st);
+  if (e != cudaSuccess) return cuda_err(e, "kernel start event");
   int rc = launch_match(labeled, graph_view(g), g->ctl, d, g->queue, queue_hdr(g), s.cfg, s.blocks,
                         s.warps_per_block, st);
   if (rc) return rc;
+  e = cudaEventRecord(k1, st);
+  if (e != cudaSuccess) return cuda_err(e, "kernel end event");
   e = cudaMemcpyAsync(h->hot, d->hot, sizeof(SlotHot) * n, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(g->hctl, g->ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) return cuda_err(e, "read-back");
   return TDFS_OK;
 }
 
-int collect(tdfs_graph *g, int n, unsigned long long *raw) {
-  const RunCtl &hc = *g->hctl;
+// Counts of a finished launch from the read-back slot lines.  A slot that ran
+// out of its work budget gets status TDFS_ERR_TIMEOUT and count 0; without a
+// status array that fails the call.
+int collect(const RunCtl &hc, const SlotHot *hot, int n, unsigned long long *raw, int *status) {
   if (hc.error == TDFS_ERR_TIMEOUT) return fail(TDFS_ERR_TIMEOUT, "a bounded device wait ran out");
   if (hc.error) return fail(hc.error, "device error %d", hc.error);
+  int first_abort = -1;
   for (int i = 0; i < n; ++i) {
-    if (g->htab->hot[i].state != kSlotDone) return fail(TDFS_ERR_TIMEOUT, "slot %d did not complete", i);
-    raw[i] = g->htab->hot[i].count;
+    if (hot[i].state != kSlotDone) return fail(TDFS_ERR_TIMEOUT, "slot %d did not complete", i);
+    const bool ab = hot[i].aborted != 0;
+    raw[i] = ab ? 0 : hot[i].count;
+    if (status) status[i] = ab ? TDFS_ERR_TIMEOUT : TDFS_OK;
+    if (ab && first_abort < 0) first_abort = i;
   }
+  if (first_abort >= 0 && !status)
+    return fail(TDFS_ERR_TIMEOUT, "pattern %d ran out of its work budget", first_abort);
   return TDFS_OK;
 }
 
-int run_captured(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, float *ms, unsigned long long *raw) {
+int run_captured(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, float *ms, unsigned long long *raw,
+                 int *status) {
   cudaError_t e;
-  if (!g->gstream) {
+  if (!g->ws->gstream) {
     cudaStream_t st;
     e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_err(e, "capture stream");
-    g->gstream = st;
+    g->ws->gstream = st;
   }
-  cudaStream_t st = static_cast<cudaStream_t>(g->gstream);
+  cudaStream_t st = static_cast<cudaStream_t>(g->ws->gstream);
   auto &cache = graph_cache(g);
-  cudaGraphExec_t exec = nullptr;
+  const GraphEntry *hit = nullptr;
   for (auto &c : cache)
     if (c.n == n && c.labeled == labeled && c.blocks == s.blocks && c.warps == s.warps_per_block &&
         !std::memcmp(&c.cfg, &s.cfg, sizeof c.cfg))
-      exec = c.exec;
-  if (!exec) {
+      hit = &c;
+  if (!hit) {
+    GraphEntry ent{n, labeled, s.blocks, s.warps_per_block, s.cfg, nullptr, nullptr, nullptr};
+    e = cudaEventCreate(&ent.k0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ent.k1);
+    if (e != cudaSuccess) return cuda_err(e, "cudaEventCreate");
     cudaGraph_t graph;
     e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) return cuda_err(e, "cudaStreamBeginCapture");
-    int rc = enqueue_launch(g, s, labeled, n, st);
+    int rc = enqueue_launch(g, s, labeled, n, st, ent.k0, ent.k1);
     e = cudaStreamEndCapture(st, &graph);
-    if (rc) return rc;
-    if (e != cudaSuccess) return cuda_err(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return cuda_err(e, "cudaGraphInstantiate");
-    cache.push_back(GraphEntry{n, labeled, s.blocks, s.warps_per_block, s.cfg, exec});
+    if (!rc && e == cudaSuccess) {
+      e = cudaGraphInstantiate(&ent.exec, graph, 0);
+      cudaGraphDestroy(graph);
+    }
+    if (rc || e != cudaSuccess) {
+      cudaEventDestroy(ent.k0);
+      cudaEventDestroy(ent.k1);
+      return rc ? rc : cuda_err(e, "capturing the launch");
+    }
+    cache.push_back(ent);
+    hit = &cache.back();
   }
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  if (ms) {
-    cudaEventCreate(&ev0);
-    cudaEventCreate(&ev1);
-    cudaEventRecord(ev0, st);
-  }
-  e = cudaGraphLaunch(exec, st);
-  if (ms) cudaEventRecord(ev1, st);
+  e = cudaGraphLaunch(hit->exec, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess && ms) e = cudaEventElapsedTime(ms, ev0, ev1);
-  if (ev0) cudaEventDestroy(ev0);
-  if (ev1) cudaEventDestroy(ev1);
+  // the match kernel's own time, from the event nodes around it in the graph
+  if (e == cudaSuccess && ms) e = cudaEventElapsedTime(ms, hit->k0, hit->k1);
   if (e != cudaSuccess) return cuda_err(e, "graph launch");
-  return collect(g, n, raw);
+  return collect(*g->hctl, g->htab->hot, n, raw, status);
 }
 
 // One launch over n plans of the same mode: slot i counts plans[i] on the
 // option's edge range; raw[i] receives the count before the |Aut| multiplier.
 int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_options &o, unsigned long long *raw,
-              float *ms) {
+              int *status, float *ms) {
   if (n <= 0) return TDFS_OK;
   if (n > kMaxSlots) return fail(TDFS_ERR_CAPACITY, "at most %d plans per launch", kMaxSlots);
   const bool labeled = plans[0]->labeled != 0;
@@ -225,6 +267,7 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   LaunchShape s;
   int rc = launch_shape(g, kmax, labeled, o, &s);
   if (rc) return rc;
+  if ((rc = acquire_workspace(g))) return rc;
   const int64_t eb = std::max<int64_t>(0, o.edge_begin);
   const int64_t ee = (o.edge_end < 0 || o.edge_end > g->nedges) ? g->nedges : o.edge_end;
   const int stride = o.edge_stride > 0 ? o.edge_stride : 1;
@@ -242,12 +285,13 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
     in.phase = o.edge_phase;
     in.chunk = chunk;
     in.ntickets = ticket_count(in.e_begin, in.e_end, stride, o.edge_phase, chunk);
+    in.budget = o.work_budget;
     std::memset(&h->hot[i], 0, sizeof h->hot[i]);
     h->hot[i].state = in.ntickets > 0 ? kSlotActive : kSlotDone;  // an empty range is done at once
     if (in.ntickets == 0) ++h->ctl.completed;
     h->plan[i] = *plans[i];
   }
-  if (o.graph_capture) return run_captured(g, s, labeled, n, ms, raw);
+  if (o.graph_capture) return run_captured(g, s, labeled, n, ms, raw, status);
   cudaStream_t st = static_cast<cudaStream_t>(o.stream);
   SlotTable *d = g->tab;
   e = cudaMemcpyAsync(&d->ctl, &h->ctl, sizeof h->ctl, cudaMemcpyHostToDevice, st);
@@ -278,13 +322,7 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (rc) return rc;
-  if (hc.error == TDFS_ERR_TIMEOUT) return fail(TDFS_ERR_TIMEOUT, "a bounded device wait ran out");
-  if (hc.error) return fail(hc.error, "device error %d", hc.error);
-  for (int i = 0; i < n; ++i) {
-    if (h->hot[i].state != kSlotDone) return fail(TDFS_ERR_TIMEOUT, "slot %d did not complete", i);
-    raw[i] = h->hot[i].count;
-  }
-  return TDFS_OK;
+  return collect(hc, h->hot, n, raw, status);
 }
 
 }  // namespace
@@ -395,7 +433,7 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
   if (opt) o = *opt; else tdfs_options_default(&o);
   unsigned long long raw = 0;
   const DevPlan *dp = &p->dev;
-  int rc = run_batch(g, &dp, 1, o, &raw, kernel_ms);
+  int rc = run_batch(g, &dp, 1, o, &raw, nullptr, kernel_ms);
   if (rc) return rc;
   // cu_test.cu:100-105: the unlabeled total is multiplied by |Aut|
   *count = (uint64_t)(raw * (unsigned long long)p->dev.multiplicity);
@@ -404,6 +442,11 @@ int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint6
 
 int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *opt,
                      uint64_t *counts, float *kernel_ms) {
+  return tdfs_count_batch_status(g, plans, nplans, opt, counts, nullptr, kernel_ms);
+}
+
+int tdfs_count_batch_status(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *opt,
+                            uint64_t *counts, int *status, float *kernel_ms) {
   if (!g || (!plans && nplans) || (!counts && nplans) || nplans < 0) return fail(TDFS_ERR_ARG, "bad arguments");
   tdfs_options o;
   if (opt) o = *opt; else tdfs_options_default(&o);
@@ -422,12 +465,15 @@ int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, c
     for (size_t b = 0; b < dp.size(); b += kMaxSlots) {
       const int n = (int)std::min<size_t>(kMaxSlots, dp.size() - b);
       std::vector<unsigned long long> raw(n);
+      std::vector<int> st(n, TDFS_OK);
       float ms = 0.f;
-      int rc = run_batch(g, dp.data() + b, n, o, raw.data(), kernel_ms ? &ms : nullptr);
+      int rc = run_batch(g, dp.data() + b, n, o, raw.data(), status ? st.data() : nullptr, kernel_ms ? &ms : nullptr);
       if (rc) return rc;
       total += ms;
-      for (int j = 0; j < n; ++j)
+      for (int j = 0; j < n; ++j) {
         counts[idx[b + j]] = (uint64_t)(raw[j] * (unsigned long long)dp[b + j]->multiplicity);
+        if (status) status[idx[b + j]] = st[j];
+      }
     }
   }
   if (kernel_ms) *kernel_ms = total;
@@ -503,6 +549,58 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
   cur.edge_phase = b.edge_phase;
   *best = cur;
   if (best_ms) *best_ms = cur_ms;
+  return TDFS_OK;
+}
+
+int tdfs_selftest_wait_limit(tdfs_graph *g, int wait_limit_ms, float *kernel_ms) {
+  if (!g || wait_limit_ms <= 0 || wait_limit_ms > 60000) return fail(TDFS_ERR_ARG, "wait_limit_ms must lie in [1, 60000]");
+  cudaError_t e = cudaSetDevice(g->device);
+  if (e != cudaSuccess) return cuda_err(e, "cudaSetDevice");
+  tdfs_options o;
+  tdfs_options_default(&o);
+  o.wait_limit_ms = wait_limit_ms;
+  LaunchShape s;
+  int rc = launch_shape(g, 3, false, o, &s);
+  if (rc) return rc;
+  if ((rc = acquire_workspace(g))) return rc;
+  // one admitted slot that no warp can ever complete: active, no tickets,
+  // no holds -- every warp finds no work and waits until its bound runs out
+  SlotTable *h = g->htab, *d = g->tab;
+  std::memset(&h->ctl, 0, sizeof h->ctl);
+  h->ctl.admitted = 1;
+  h->ctl.shutdown = 1;
+  std::memset(&h->hot[0], 0, sizeof h->hot[0]);
+  h->hot[0].state = kSlotActive;
+  std::memset(&h->info[0], 0, sizeof h->info[0]);
+  h->info[0].stride = 1;
+  h->info[0].chunk = 1;
+  DevPlan p;
+  std::memset(&p, 0, sizeof p);
+  p.k = 3;
+  h->plan[0] = p;
+  e = cudaMemcpy(&d->ctl, &h->ctl, sizeof h->ctl, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d->hot, h->hot, sizeof(SlotHot), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d->info, h->info, sizeof(SlotInfo), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d->plan, h->plan, sizeof(DevPlan), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_err(e, "slot upload");
+  cudaEvent_t ev0, ev1;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  init_launch(g->ctl, queue_hdr(g), nullptr);
+  cudaEventRecord(ev0, nullptr);
+  rc = launch_match(false, graph_view(g), g->ctl, d, g->queue, queue_hdr(g), s.cfg, s.blocks, s.warps_per_block,
+                    nullptr);
+  cudaEventRecord(ev1, nullptr);
+  RunCtl hc;
+  if (!rc) {
+    e = cudaMemcpy(&hc, g->ctl, sizeof hc, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && kernel_ms) e = cudaEventElapsedTime(kernel_ms, ev0, ev1);
+    if (e != cudaSuccess) rc = cuda_err(e, "self-test launch");
+  }
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  if (rc) return rc;
+  if (hc.error) return fail(hc.error, "the launch reported device status %d after its bounded waits", hc.error);
   return TDFS_OK;
 }
 

@@ -9,9 +9,10 @@
 //   tdfs_convert labels  <prefix> <nlabels> <seed>   (writes <prefix>.label.bin)
 //   tdfs_convert relabel <in prefix> <out prefix>    (graph_converter/relabel.cpp)
 //   tdfs_convert halve   <in prefix> <out prefix>    (graph_converter/halve.cpp)
+//   tdfs_convert pattern <k> <density> <nlabels> <seed>   (prints a .g pattern)
 //
-// Prints "n E max_degree" of the written graph.  Errors go to stderr with
-// exit status 1.
+// Prints "n E max_degree" of the written graph (the pattern text for
+// `pattern`).  Errors go to stderr with exit status 1.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -28,8 +29,9 @@ int usage(const char *argv0) {
                "       %s rmat <scale> <edge_factor> <a> <b> <c> <seed> <out>\n"
                "       %s labels <prefix> <nlabels> <seed>\n"
                "       %s relabel <in> <out>\n"
-               "       %s halve <in> <out>\n",
-               argv0, argv0, argv0, argv0, argv0, argv0);
+               "       %s halve <in> <out>\n"
+               "       %s pattern <k> <density> <nlabels> <seed>\n",
+               argv0, argv0, argv0, argv0, argv0, argv0, argv0);
   return 2;
 }
 
@@ -51,6 +53,17 @@ int main(int argc, char **argv) {
   tdfs_csr *c = nullptr, *d = nullptr;
   int rc = 0;
   const char *out = nullptr;
+  if (cmd == "pattern" && argc == 6) {
+    char buf[1024];
+    rc = tdfs_gen_pattern(std::atoi(argv[2]), std::atof(argv[3]), std::atoi(argv[4]),
+                          std::strtoull(argv[5], nullptr, 10), buf, sizeof buf);
+    if (rc) {
+      std::fprintf(stderr, "%s\n", tdfs_last_error());
+      return 1;
+    }
+    std::fputs(buf, stdout);
+    return 0;
+  }
   if (cmd == "er" && argc == 6) {
     rc = tdfs_gen_er(std::atoll(argv[2]), std::atof(argv[3]), std::strtoull(argv[4], nullptr, 10), &c);
     out = argv[5];

@@ -29,10 +29,13 @@ int hw_threads() {
   return t ? (int)std::min(t, 64u) : 4;
 }
 
+// f(b, e) over [0, n) split across host threads; `work` (default n) is the
+// total cost in elementary steps: below ~2M steps one thread does it all,
+// since starting threads would cost more than they save.
 template <class F>
-void parallel_for(int64_t n, F f) {
+void parallel_for(int64_t n, F f, int64_t work = -1) {
   int T = hw_threads();
-  if (n < 4096) T = 1;
+  if ((work < 0 ? n : work) < (1 << 21)) T = 1;
   std::vector<std::thread> th;
   for (int t = 0; t < T; ++t)
     th.emplace_back([=] {
@@ -70,7 +73,8 @@ int validate_csr(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   std::atomic<int64_t> where{-1};
   std::vector<int32_t> part_max(hw_threads() + 1, 0);
   std::atomic<int> slot{0};
-  parallel_for(n, [&](int64_t b, int64_t e) {
+  parallel_for(
+      n, [&](int64_t b, int64_t e) {
     int32_t md = 0;
     for (int64_t v = b; v < e && !bad.load(std::memory_order_relaxed); ++v) {
       int64_t lo = rowptr[v], hi = rowptr[v + 1];
@@ -83,7 +87,7 @@ int validate_csr(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
       }
     }
     part_max[slot++] = md;
-  });
+  }, n + nedges);
   if (bad == 1) return fail(TDFS_ERR_FORMAT, "rowptr decreases at vertex %lld", (long long)where.load());
   if (bad == 2) return fail(TDFS_ERR_FORMAT, "neighbour id out of range in row %lld", (long long)where.load());
   if (bad == 3)

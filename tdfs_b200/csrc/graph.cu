@@ -13,7 +13,9 @@
 //   label   uint8[n]          labeled graphs only (labels must be < 255)
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "csr.h"
@@ -82,46 +84,121 @@ int prepare_graph_arrays(const int64_t *rowptr, const int32_t *colidx, int32_t n
   return e == cudaSuccess ? TDFS_OK : cuda_fail(e, "graph preparation kernels");
 }
 
-#define CK(x)                                    \
-  do {                                           \
-    cudaError_t e_ = (x);                        \
-    if (e_ != cudaSuccess) {                     \
-      release(g);                                \
-      delete g;                                  \
-      return cuda_fail(e_, #x);                  \
-    }                                            \
-  } while (0)
+namespace {
 
-void release(tdfs_graph *g) {
-  if (!g) return;
-  cudaFree(g->rowptr);
-  cudaFree(g->colidx);
-  cudaFree(g->src);
-  cudaFree(g->maxnd);
-  cudaFree(g->label);
-  cudaFree(g->ctl);
-  cudaFree(g->queue);
-  cudaFree(g->tab);
-  if (g->htab) cudaFreeHost(g->htab);
-  if (g->hctl) cudaFreeHost(g->hctl);
-  g->hctl = nullptr;
-  g->tab = nullptr;
-  g->htab = nullptr;
-  g->rowptr = nullptr;
-  g->colidx = nullptr;
-  g->src = nullptr;
-  g->maxnd = nullptr;
-  g->label = nullptr;
-  g->ctl = nullptr;
-  g->queue = nullptr;
+// ---- launch workspaces, pooled per device ---------------------------------
+std::mutex g_pool_mu;
+std::vector<Workspace *> g_pool;        // idle workspaces (any device)
+constexpr int kIdlePerDevice = 4;       // idle workspaces kept per device; more are freed
+
+void free_workspace(Workspace *w) {
+  cudaFree(w->ctl);
+  cudaFreeHost(w->htab);
+  if (w->gstream) cudaStreamDestroy(static_cast<cudaStream_t>(w->gstream));
+  delete w;
 }
 
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+
+int acquire_workspace(tdfs_graph *g) {
+  if (g->ws) return TDFS_OK;
+  Workspace *w = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (size_t i = 0; i < g_pool.size(); ++i)
+      if (g_pool[i]->device == g->device) {
+        w = g_pool[i];
+        g_pool.erase(g_pool.begin() + (long)i);
+        break;
+      }
+  }
+  if (!w) {
+    // one device allocation (control block, ring, slot table) and one pinned
+    // host allocation (staging copies of the slot table and control block)
+    const size_t o_queue = align256(sizeof(RunCtl));
+    const size_t o_tab = o_queue + align256(sizeof(SplitUnit) * kQueueCap + sizeof(QueueHdr));
+    const size_t dev_bytes = o_tab + align256(sizeof(SlotTable));
+    const size_t o_hctl = align256(sizeof(SlotTable));
+    w = new Workspace{};
+    w->device = g->device;
+    char *d = nullptr, *h = nullptr;
+    cudaError_t e = cudaMalloc(&d, dev_bytes);
+    if (e == cudaSuccess) {
+      e = cudaMallocHost(&h, o_hctl + sizeof(RunCtl));
+      if (e != cudaSuccess) cudaFree(d);
+    }
+    if (e != cudaSuccess) {
+      delete w;
+      return cuda_fail(e, "launch workspace");
+    }
+    w->ctl = reinterpret_cast<RunCtl *>(d);
+    w->queue = reinterpret_cast<SplitUnit *>(d + o_queue);
+    w->tab = reinterpret_cast<SlotTable *>(d + o_tab);
+    w->htab = reinterpret_cast<SlotTable *>(h);
+    w->hctl = reinterpret_cast<RunCtl *>(h + o_hctl);
+  }
+  g->ws = w;
+  g->ctl = w->ctl;
+  g->queue = w->queue;
+  g->tab = w->tab;
+  g->htab = w->htab;
+  g->hctl = w->hctl;
+  return TDFS_OK;
+}
+
+namespace {
+
+void release_workspace(tdfs_graph *g) {
+  Workspace *w = g->ws;
+  if (!w) return;
+  g->ws = nullptr;
+  g->ctl = nullptr;
+  g->queue = nullptr;
+  g->tab = nullptr;
+  g->htab = nullptr;
+  g->hctl = nullptr;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  int idle = 0;
+  for (Workspace *x : g_pool) idle += x->device == w->device;
+  if (idle < kIdlePerDevice) g_pool.push_back(w);
+  else free_workspace(w);
+}
+
+}  // namespace
+
+// The graph arrays live in one device allocation:
+//   rowptr int64[n+1] | colidx int32[E + kColPad] | src int32[E] | maxnd int32[n] | label uint8[n]
+// each part starting on a 256-byte boundary.  Labels are checked and
+// narrowed to 8 bits on the host, so the upload is a few stream-ordered
+// copies and two preprocessing kernels, synchronised once at the end.
 int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx, const int32_t *labels,
                  int device, int32_t max_degree, tdfs_graph **out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(TDFS_ERR_CUDA, "no CUDA device visible (the tdfs engine has no CPU path)");
   if (device < 0 || device >= ndev) return fail(TDFS_ERR_ARG, "device %d out of range", device);
+  std::vector<uint8_t> lab8;
+  if (labels) {
+    lab8.resize((size_t)n);
+    for (int64_t i = 0; i < n; ++i) {
+      if (labels[i] < 0 || labels[i] > 254)
+        return fail(TDFS_ERR_FORMAT, "vertex labels must lie in [0, 254] for the device label array");
+      lab8[(size_t)i] = (uint8_t)labels[i];
+    }
+  }
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  static_assert(kColPad % 4 == 0, "padding keeps 16-byte loads aligned");
+  const size_t o_col = align256(sizeof(int64_t) * (size_t)(n + 1));
+  const size_t o_src = o_col + align256(sizeof(int32_t) * (size_t)(nedges + kColPad));
+  const size_t o_maxnd = o_src + align256(sizeof(int32_t) * (size_t)(nedges ? nedges : 1));
+  const size_t o_label = o_maxnd + align256(sizeof(int32_t) * (size_t)(n ? n : 1));
+  const size_t total = o_label + align256((size_t)(labels && n ? n : 1));
+  char *base = nullptr;
+  e = cudaMalloc(&base, total);
+  if (e != cudaSuccess) return cuda_fail(e, "graph arrays");
   auto *g = new tdfs_graph;
   std::memset(g, 0, sizeof *g);
   g->device = device;
@@ -129,52 +206,37 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   g->nedges = nedges;
   g->max_degree = max_degree;
   g->labeled = labels != nullptr;
-  cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) {
-    delete g;
-    return cuda_fail(e, "cudaSetDevice");
-  }
-  static_assert(kColPad % 4 == 0, "padding keeps 16-byte loads aligned");
-  CK(cudaMalloc(&g->rowptr, sizeof(int64_t) * (n + 1)));
-  CK(cudaMalloc(&g->colidx, sizeof(int32_t) * (nedges + kColPad)));
-  CK(cudaMalloc(&g->src, sizeof(int32_t) * (nedges ? nedges : 1)));
-  CK(cudaMalloc(&g->maxnd, sizeof(int32_t) * (n ? n : 1)));
-  CK(cudaMalloc(&g->ctl, sizeof(RunCtl)));
-  CK(cudaMalloc(&g->queue, sizeof(SplitUnit) * kQueueCap + sizeof(QueueHdr)));
-  CK(cudaMalloc(&g->tab, sizeof(SlotTable)));
-  CK(cudaMallocHost(&g->htab, sizeof(SlotTable)));
-  CK(cudaMallocHost(&g->hctl, sizeof(RunCtl)));
-  CK(cudaMemcpy(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(g->colidx, colidx, sizeof(int32_t) * nedges, cudaMemcpyHostToDevice));
-  CK(cudaMemset(g->colidx + nedges, 0x7f, sizeof(int32_t) * kColPad));
-  g->bytes = sizeof(int64_t) * (n + 1) + sizeof(int32_t) * (2 * nedges + kColPad + n);
-  if (n > 0) {
+  g->arrays = base;
+  g->rowptr = reinterpret_cast<int64_t *>(base);
+  g->colidx = reinterpret_cast<int32_t *>(base + o_col);
+  g->src = reinterpret_cast<int32_t *>(base + o_src);
+  g->maxnd = reinterpret_cast<int32_t *>(base + o_maxnd);
+  g->label = labels ? reinterpret_cast<uint8_t *>(base + o_label) : nullptr;
+  g->bytes = total;
+  const cudaStream_t st = cudaStreamPerThread;
+  e = cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nedges)
+    e = cudaMemcpyAsync(g->colidx, colidx, sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->colidx + nedges, 0x7f, sizeof(int32_t) * kColPad, st);
+  if (e == cudaSuccess && labels && n)
+    e = cudaMemcpyAsync(g->label, lab8.data(), (size_t)n, cudaMemcpyHostToDevice, st);
+  int rc = TDFS_OK;
+  if (e == cudaSuccess && n > 0) {
     const int threads = 256;
     const int64_t want = ((int64_t)n * 32 + threads - 1) / threads;
     const int blocks = (int)std::min<int64_t>(want, 148 * 16);
-    build_src_kernel<<<blocks, threads>>>(g->rowptr, (int32_t)n, g->src);
-    max_nbr_deg_kernel<<<blocks, threads>>>(g->rowptr, g->colidx, (int32_t)n, g->maxnd);
-    CK(cudaGetLastError());
+    build_src_kernel<<<blocks, threads, 0, st>>>(g->rowptr, (int32_t)n, g->src);
+    max_nbr_deg_kernel<<<blocks, threads, 0, st>>>(g->rowptr, g->colidx, (int32_t)n, g->maxnd);
+    e = cudaGetLastError();
   }
-  if (labels) {
-    int32_t *tmp = nullptr, *bad = nullptr;
-    CK(cudaMalloc(&g->label, n ? n : 1));
-    CK(cudaMalloc(&tmp, sizeof(int32_t) * (n + 1)));
-    bad = tmp + n;
-    CK(cudaMemcpy(tmp, labels, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-    CK(cudaMemset(bad, 0, sizeof(int32_t)));
-    if (n > 0) narrow_labels_kernel<<<148 * 4, 256>>>(tmp, (int32_t)n, g->label, bad);
-    int32_t hbad = 0;
-    CK(cudaMemcpy(&hbad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost));
-    cudaFree(tmp);
-    if (hbad) {
-      release(g);
-      delete g;
-      return fail(TDFS_ERR_FORMAT, "vertex labels must lie in [0, 254] for the device label array");
-    }
-    g->bytes += n;
+  // the host label copy and the caller's arrays must outlive the copies
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) rc = cuda_fail(e, "graph upload");
+  if (rc) {
+    cudaFree(base);
+    delete g;
+    return rc;
   }
-  CK(cudaDeviceSynchronize());
   *out = g;
   return TDFS_OK;
 }
@@ -185,9 +247,8 @@ void graph_release(tdfs_graph *g) {
   cudaGetDevice(&cur);
   cudaSetDevice(g->device);
   release_graphs(g);
-  if (g->gstream) cudaStreamDestroy(static_cast<cudaStream_t>(g->gstream));
-  g->gstream = nullptr;
-  release(g);
+  release_workspace(g);
+  cudaFree(g->arrays);
   cudaSetDevice(cur);
   delete g;
 }

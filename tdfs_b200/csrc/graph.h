@@ -41,7 +41,7 @@ struct alignas(128) QueueHdr {
 // filled by the host before the kernel may see them (`admitted`) and are never
 // reused within one launch, so a warp holding a stale slot index can only
 // touch a finished slot, never a recycled one.
-constexpr int kMaxSlots = 4096;
+constexpr int kMaxSlots = 16384;
 
 enum : int32_t { kSlotEmpty = 0, kSlotActive = 1, kSlotDone = 2 };
 
@@ -53,6 +53,8 @@ struct alignas(128) SlotHot {
   int32_t state;              // kSlotActive -> kSlotDone (by the completing warp)
   unsigned long long t_first; // globaltimer when the first ticket was taken
   unsigned long long t_done;  // globaltimer at completion
+  unsigned long long work;    // work units spent so far (flushed by warps; budgeted launches)
+  int32_t aborted;            // 1: the work budget ran out; the count is not valid
 };
 
 // Written by the host at admission, read-only for the kernel.
@@ -61,8 +63,9 @@ struct SlotInfo {
   int64_t e_end;
   int64_t ntickets;  // tickets of this slot
   int32_t stride, phase;
-  int32_t chunk;     // directed edges per ticket (8, 16 or 32)
+  int32_t chunk;     // directed edges per ticket (1, 2, 4, ..., 32)
   int32_t pad_;
+  int64_t budget;    // work units this query may spend (0 = unlimited)
 };
 
 struct alignas(128) SlotCtl {
@@ -86,23 +89,44 @@ struct SlotTable {
 
 }  // namespace tdfs
 
+namespace tdfs {
+
+// Launch workspace: what one persistent launch needs besides the graph --
+// the control block, the split ring, the slot table and its pinned host
+// staging copy.  About 12 MB of device memory and 1.7 MB of pinned host
+// memory, so it is pooled per device (graph.cu) instead of being allocated
+// with every graph: a graph takes one at its first launch and hands it back
+// when it is freed.
+struct Workspace {
+  int device;
+  RunCtl *ctl;
+  SplitUnit *queue;    // split-unit ring: kQueueCap units then a QueueHdr
+  SlotTable *tab;
+  SlotTable *htab;     // pinned
+  RunCtl *hctl;        // pinned
+  void *gstream;       // cudaStream_t for captured launches (created on first use)
+};
+
+}  // namespace tdfs
+
 struct tdfs_graph {
   int device;
   int64_t n;
   int64_t nedges;
   int32_t max_degree;
   bool labeled;
+  void *arrays;           // the one device allocation holding the arrays below
   int64_t *rowptr;
   int32_t *colidx;
   int32_t *src;
   int32_t *maxnd;
   uint8_t *label;
-  tdfs::RunCtl *ctl;     // launch control block (one launch at a time per handle)
-  tdfs::SplitUnit *queue; // split-unit ring: kQueueCap units then a QueueHdr
-  tdfs::SlotTable *tab;   // query slots of a launch
-  tdfs::SlotTable *htab;  // pinned host staging copy of the slot table
-  tdfs::RunCtl *hctl;     // pinned host copy of the control block
-  void *gstream;          // cudaStream_t for captured launches (created on first use)
+  tdfs::Workspace *ws;    // launch workspace (pooled; taken at the first launch)
+  tdfs::RunCtl *ctl;      // = ws->ctl etc. while a workspace is held
+  tdfs::SplitUnit *queue;
+  tdfs::SlotTable *tab;
+  tdfs::SlotTable *htab;
+  tdfs::RunCtl *hctl;
   void *graphs;           // cache of instantiated launch graphs (capi.cpp)
   size_t bytes;
 };
@@ -112,6 +136,9 @@ namespace tdfs {
 int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx, const int32_t *labels,
                  int device, int32_t max_degree, tdfs_graph **out);
 void graph_release(tdfs_graph *g);
+// Give g a launch workspace from its device's pool (allocating one when none
+// is idle); the device must be current.  Idempotent.
+int acquire_workspace(tdfs_graph *g);
 void release_graphs(tdfs_graph *g);  // capi.cpp: destroys cached launch graphs
 DevGraph graph_view(const tdfs_graph *g);
 int prepare_graph_arrays(const int64_t *rowptr, const int32_t *colidx, int32_t n, const int32_t *labels,

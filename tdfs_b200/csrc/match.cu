@@ -23,6 +23,7 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMaxLists = kMaxK - 1;
 constexpr int kCasLimit = 1 << 20;
 constexpr int kStoredMax = kMaxK;  // level index bound (stored levels are 2..k-2)
+constexpr int kFlatUnroll = 4;     // positions per lane in flight in the flattened last-level pass
 
 struct LevelHdr {
   const int32_t *src;            // source list: global adjacency list or an smem buffer
@@ -183,6 +184,7 @@ struct Engine {
   unsigned char *cta;   // this CTA's shared memory (warp regions cfg.warp_bytes apart)
   size_t hdr_bytes;     // WarpSmem rounded to 16 bytes
   unsigned long long count = 0;
+  unsigned long long work = 0;  // work units since the last flush: one per claim and per 32-wide scan step
   int lane;
 
   __device__ Engine(const DevGraph &g, const KernelCfg &c, RunCtl *ct, SlotTable *tb, SplitUnit *u, QueueHdr *q,
@@ -332,6 +334,7 @@ struct Engine {
       if (ok) out[n + __popc(mask & lanemask_lt())] = x;
       n += __popc(mask);
       spos += 32;
+      ++work;
     }
     __syncwarp();
     if (lane == 0) {
@@ -379,6 +382,7 @@ struct Engine {
     int32_t n = 0;
     bool over = false;
     for (int32_t spos = H.spos; spos < send; spos += 32) {
+      ++work;
       if (n > cfg.cap - 32) {  // a full step could write past the buffer: give up
         over = true;
         break;
@@ -419,12 +423,16 @@ struct Engine {
     return LAB ? 0 : (P.larger[i] >> (i - 1) & 1) ? 1 : (P.less[i] >> (i - 1) & 1) ? 2 : 0;
   }
 
-  // Last level over a batch of b parents (items[0..b), b <= 32) that share
-  // the fixed set F: lane j counts |F ∩ N(items[j])| by itself when that list
-  // is at most cfg.lane_list long -- 32 short lists at once, their memory
-  // latencies overlapped, instead of one warp-wide pass per parent with most
-  // lanes idle -- and the longer lists are counted by the whole warp after.
-  __device__ unsigned long long count_fixed_batch(int i, const int32_t *items, int b) {
+  // Last level over a batch of b siblings (items[0..b), b <= 32) that share
+  // the fixed set F, in one flattened warp-wide pass: the siblings' adjacency
+  // lists are laid end to end (an exclusive scan of their lengths) and lane t
+  // takes positions t, t + 32, ... of that sequence, kFlatUnroll positions at
+  // once, so the loads are coalesced within each list and several rounds of
+  // them are in flight together -- one pass over the batch instead of a
+  // dependent rowptr -> list -> search chain per sibling.  Lists longer than
+  // max(cfg.lane_list, 4 |F|) (hubs) are counted one by one afterwards by
+  // count_fixed_list, which searches F's elements in them instead.
+  __device__ unsigned long long count_fixed_flat(int i, const int32_t *items, int b) {
     const int32_t *F = fbuf();
     const int32_t nF = W.fn;
     if (nF == 0) return 0;
@@ -436,27 +444,89 @@ struct Engine {
       rb = G.rowptr[x];
       re = G.rowptr[x + 1];
     }
-    const bool alone = mine && re - rb <= (int64_t)cfg.lane_list;
+    const int64_t lim = cfg.lane_list > 4 * nF ? (int64_t)cfg.lane_list : 4ll * nF;
+    const bool flat = mine && re - rb <= lim;
+    const int32_t len = flat ? (int32_t)(re - rb) : 0;
+    int32_t incl = len;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+      const int32_t t = __shfl_up_sync(kFull, incl, s);
+      if (lane >= s) incl += t;
+    }
+    const int32_t off = incl - len;  // exclusive prefix: first position of this lane's list
+    const int32_t total = __shfl_sync(kFull, incl, 31);
     unsigned c = 0;
-    if (alone) {
-      const int32_t *L = G.colidx + rb;
-      const int32_t len = (int32_t)(re - rb);
-      int32_t q = 0;  // F cursor: L is sorted, so each search starts where the last ended
-      for (int32_t t = 0; t < len && q < nF; ++t) {
-        const int32_t y = L[t];
-        if (rel == 1 ? y <= x : rel == 2 ? y >= x : y == x) continue;
-        q = lower_bound(F, q, nF, y);
-        c += q < nF && F[q] == y;
+    for (int32_t base = 0; base < total; base += 32 * kFlatUnroll) {
+      work += kFlatUnroll;
+      int32_t y[kFlatUnroll], xo[kFlatUnroll];
+      bool v[kFlatUnroll];
+#pragma unroll
+      for (int u = 0; u < kFlatUnroll; ++u) {
+        const int32_t pos = base + u * 32 + lane;
+        // owner: the last sibling whose list starts at or before pos
+        int j = 0;
+#pragma unroll
+        for (int s = 16; s >= 1; s >>= 1) {
+          const int32_t oc = __shfl_sync(kFull, off, j + s);
+          if (oc <= pos) j += s;
+        }
+        const int32_t oj = __shfl_sync(kFull, off, j);
+        const int64_t bj = __shfl_sync(kFull, rb, j);
+        xo[u] = __shfl_sync(kFull, x, j);
+        v[u] = pos < total;
+        y[u] = v[u] ? G.colidx[bj + (pos - oj)] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < kFlatUnroll; ++u) {
+        const int32_t yy = y[u], xx = xo[u];
+        if (v[u] && (rel == 1 ? yy > xx : rel == 2 ? yy < xx : yy != xx)) {
+          const int32_t q = lower_bound(F, 0, nF, yy);
+          c += q < nF && F[q] == yy;
+        }
       }
     }
-    unsigned long long total = __reduce_add_sync(kFull, c);
-    unsigned rest = __ballot_sync(kFull, mine && !alone);
+    unsigned long long sum = __reduce_add_sync(kFull, c);
+    unsigned rest = __ballot_sync(kFull, mine && !flat);
     while (rest) {
       const int j = __ffs(rest) - 1;
       rest &= rest - 1;
-      total += count_fixed_list(i, __shfl_sync(kFull, x, j), __shfl_sync(kFull, rb, j), __shfl_sync(kFull, re, j));
+      sum += count_fixed_list(i, __shfl_sync(kFull, x, j), __shfl_sync(kFull, rb, j), __shfl_sync(kFull, re, j));
     }
-    return total;
+    return sum;
+  }
+
+  // The last vertex i when its parent (vertex i-1) is not one of its backward
+  // neighbours: its whole candidate set C (F, built once per grandparent by
+  // build_fixed with every condition except the one on the parent) is the
+  // same for all siblings at level i-1, and sibling x counts the elements of
+  // C that satisfy that one condition: y > x, y < x, or y != x (unlabeled
+  // symmetry conditions, or injectivity when labeled).  C is sorted, so each
+  // sibling is one binary search in shared memory; lane j takes sibling j.
+  __device__ bool free_applies(int i) {
+    if (!cfg.fixed || i < 3) return false;
+    for (int t = 0; t < P.nbn[i]; ++t)
+      if (P.bn[i][t] == i - 1) return false;
+    return true;
+  }
+
+  __device__ unsigned long long count_free_batch(int i, const int32_t *items, int b) {
+    const int32_t *F = fbuf();
+    const int32_t nF = W.fn;
+    if (nF == 0) return 0;
+    const int rel = parent_rel(i);
+    unsigned c = 0;
+    if (lane < b) {
+      const int32_t x = items[lane];
+      if (rel == 1) {
+        c = (unsigned)(nF - upper_bound_smem(F, nF, x));
+      } else if (rel == 2) {
+        c = (unsigned)lower_bound(F, 0, nF, x);
+      } else {
+        const int32_t q = lower_bound(F, 0, nF, x);
+        c = (unsigned)(nF - (q < nF && F[q] == x ? 1 : 0));
+      }
+    }
+    return __reduce_add_sync(kFull, c);
   }
 
   // |F ∩ N(x)| under the parent condition, the warp together; N(x) is
@@ -473,6 +543,7 @@ struct Engine {
       int32_t start = 0;
       if (rel == 1 && len > 64) start = warp_upper_bound(L, 0, len, x);
       for (int32_t pos = start; pos < len; pos += 32) {
+        ++work;
         const int32_t idx = pos + lane;
         const bool valid = idx < len;
         const int32_t y = valid ? L[idx] : 0;
@@ -488,6 +559,7 @@ struct Engine {
       int32_t start = rel == 1 ? upper_bound_smem(F, nF, x) : 0;
       int32_t curp = 0;
       for (int32_t pos = start; pos < nF; pos += 32) {
+        ++work;
         const int32_t idx = pos + lane;
         const bool valid = idx < nF;
         const int32_t y = valid ? F[idx] : 0;
@@ -544,6 +616,7 @@ struct Engine {
     for (int m = 0; m < kMaxLists; ++m) cur[m] = m < H.nm ? H.mcur[m] : 0;
     unsigned long long c = 0;
     for (; spos < send; spos += 32) {
+      ++work;
       const int32_t idx = spos + lane;
       const bool valid = idx < send;
       const int32_t x = valid ? src[idx] : 0;
@@ -992,6 +1065,39 @@ struct Engine {
     __syncwarp();
   }
 
+  // ---- work budget (budgeted launches) -------------------------------------
+  // Every warp counts work units (one per claim and per 32-wide scan step) and
+  // adds them to its slot's counter every few claims.  The flush that takes
+  // the counter past the slot's budget marks the slot aborted and closes its
+  // level-0 tickets; every warp holding work of an aborted slot drops it at
+  // its next check, and the slot then completes through the usual holds with
+  // `aborted` set (its count is not valid).  Returns true when the slot this
+  // warp works on is aborted.
+  __device__ bool over_budget() {
+    int ab = 0;
+    if (lane == 0 && W.slot >= 0) {
+      const int s = W.slot;
+      SlotHot &h = tab->hot[s];
+      const long long budget = __ldcg(&tab->info[s].budget);
+      if (budget > 0) {
+        const unsigned long long tot = atomicAdd(&h.work, work) + work;
+        if ((long long)tot > budget && atomicCAS(&h.aborted, 0, 1) == 0)
+          atomicMax(&h.ticket, (unsigned long long)__ldcg(&tab->info[s].ntickets));
+        ab = *(volatile int32_t *)&h.aborted;
+      }
+    }
+    work = 0;
+    return __shfl_sync(kFull, ab, 0) != 0;
+  }
+
+  // Drop the subtree this warp holds at levels base..level: every level word
+  // gets a new generation with no items, so no thief can take them either.
+  __device__ void abandon(int base, int level) {
+    if (lane == 0)
+      for (int l = base; l <= level; ++l) publish(l, 0);
+    __syncwarp();
+  }
+
   // ---- main loop ------------------------------------------------------------
   // level 1 iterates edge pairs, 2..k-2 iterate buffered candidates, the last
   // vertex k-1 is counted in place.  `base` is the shallowest level this warp
@@ -1063,16 +1169,28 @@ struct Engine {
         if (!wait_for_work()) break;
         continue;
       }
-      if (cfg.lane_list > 0 && level >= 2 && level + 1 == P.k - 1 && fixed_applies(level + 1)) {
-        // last stored level: batches of items, short lists counted one per lane
-        if (W.fvalid == 0) build_fixed(level + 1);
-        if (W.fvalid == 1) {
-          int b = 0;
-          const int32_t first = claim_batch(level, &b);
-          if (b > 0) {
-            count += count_fixed_batch(level + 1, buf(level) + first, b);
-            if (cfg.steal) maybe_donate(level);
-            continue;
+      if (level >= 2 && level + 1 == P.k - 1) {
+        // last stored level: batches of up to 32 siblings against the fixed
+        // part of the last vertex's candidates (built once per grandparent)
+        const int i = level + 1;
+        const int mode = free_applies(i) ? 2 : (cfg.lane_list > 0 && fixed_applies(i)) ? 1 : 0;
+        if (mode) {
+          if (W.fvalid == 0) build_fixed(i);
+          if (W.fvalid == 1) {
+            int b = 0;
+            const int32_t first = claim_batch(level, &b);
+            if (b > 0) {
+              work += b;
+              if (cfg.budgeted && ((++claims & 7u) == 0) && over_budget()) {
+                abandon(base, level);
+                level = base - 1;
+                continue;
+              }
+              count += mode == 2 ? count_free_batch(i, buf(level) + first, b)
+                                 : count_fixed_flat(i, buf(level) + first, b);
+              if (cfg.steal) maybe_donate(level);
+              continue;
+            }
           }
         }
       }
@@ -1091,7 +1209,15 @@ struct Engine {
           if (lane == 0) W.phi[level] = x;
         }
         __syncwarp();
-        if (cfg.steal && ((++claims & 7u) == 0)) maybe_donate(level);
+        ++work;
+        if ((++claims & 7u) == 0) {
+          if (cfg.budgeted && over_budget()) {
+            abandon(base, level);
+            level = base - 1;
+            continue;
+          }
+          if (cfg.steal) maybe_donate(level);
+        }
         if (level + 1 == P.k - 1) {
           count += count_last(P.k - 1);
         } else {

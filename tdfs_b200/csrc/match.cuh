@@ -57,7 +57,9 @@ struct KernelCfg {
                            // (donation to the HBM ring after 4x as long)
   int32_t wide_regs;    // 1: the 80-register build (at most 3 CTAs of 256 threads per SM)
   int32_t steal_first;  // first look for levels with >= steal_first items, then the ring, then steal_min
-  int32_t lane_list;    // last level: parents with lists up to this long are counted one per lane (0 = off)
+  int32_t lane_list;    // last level: siblings' lists up to max(lane_list, 4 |F|) long go to the
+                        // flattened batch pass (0 = off: one warp pass per sibling)
+  int32_t budgeted;     // 1: some slot has a work budget (SlotInfo::budget); warps account their work
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)

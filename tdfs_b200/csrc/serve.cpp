@@ -102,6 +102,7 @@ struct Server {
   bool kernel_live = false;
   std::vector<double> latencies;
   uint64_t completed = 0;
+  uint64_t aborted = 0;
   Clock::time_point first_submit{}, last_done{};
   std::thread th;
 };
@@ -164,6 +165,7 @@ int admit(Server &S, std::vector<Pending> &batch) {
     in.phase = 0;
     in.chunk = auto_chunk(S.g->nedges, 1, S.shape.blocks * S.shape.warps_per_block, S.opt.launch.edge_chunk);
     in.ntickets = (S.g->nedges + in.chunk - 1) / in.chunk;
+    in.budget = S.opt.launch.work_budget;
     std::memset(&h->hot[s], 0, sizeof h->hot[s]);
     h->hot[s].state = kSlotActive;
     h->plan[s] = q.plan;
@@ -207,7 +209,12 @@ int poll(Server &S) {
     S.slot_done[s] = 1;
     Result &r = S.results[S.slot_ticket[s]];
     r.done = true;
-    r.count = (uint64_t)(S.mirror[s].count * (unsigned long long)S.g->htab->plan[s].multiplicity);
+    if (S.mirror[s].aborted) {
+      r.error = TDFS_ERR_TIMEOUT;  // ran out of its work budget: no valid count
+      ++S.aborted;
+    } else {
+      r.count = (uint64_t)(S.mirror[s].count * (unsigned long long)S.g->htab->plan[s].multiplicity);
+    }
     r.latency_us = std::chrono::duration<double, std::micro>(now - S.slot_submit[s]).count();
     S.latencies.push_back(r.latency_us);
     S.used_bytes -= S.slot_bytes[s];
@@ -310,6 +317,7 @@ int server_create(tdfs_graph *g, const tdfs_server_options *o, Server **out) {
   tdfs_options lo = S->opt.launch;
   int rc = launch_shape(g, S->opt.max_k, S->labeled, lo, &S->shape);
   if (rc) return rc;
+  if ((rc = acquire_workspace(g))) return rc;
   S->cap = S->shape.cfg.cap;
   if (S->opt.mem_budget == 0)
     S->opt.mem_budget = (size_t)S->opt.max_inflight * query_bytes(S->opt.max_k, S->cap, S->shape.warps_per_block);
@@ -356,6 +364,10 @@ int server_wait(Server *S, uint64_t ticket, uint64_t *count, double *latency_us)
   S->cv_done.wait(lk, [&] { return S->results[ticket].done; });
   Result r = S->results[ticket];
   S->results.erase(ticket);
+  if (latency_us) *latency_us = r.latency_us;
+  if (r.error == TDFS_ERR_TIMEOUT && !S->fatal)
+    return fail(r.error, "query %llu ran out of its work budget (%lld units)", (unsigned long long)ticket,
+                (long long)S->opt.launch.work_budget);
   if (r.error) return fail(r.error, "query failed: %s", S->fatal_msg.c_str());
   if (count) *count = r.count;
   if (latency_us) *latency_us = r.latency_us;
@@ -366,6 +378,7 @@ int server_stats(Server *S, tdfs_serve_stats *st) {
   std::lock_guard<std::mutex> lk(S->mu);
   std::memset(st, 0, sizeof *st);
   st->completed = S->completed;
+  st->aborted = S->aborted;
   st->pending = S->pending.size();
   st->inflight = S->inflight;
   std::vector<double> l = S->latencies;

@@ -1,5 +1,6 @@
-"""Host-side pieces of bench.py: the step edge ranges, the committed traffic
-record it reads into the roofline, and the clock record without nvidia-smi."""
+"""Host-side pieces of bench.py: the step edge ranges, the committed ncu
+record it reads into the roofline, the reference arm's engine-free inputs, and
+the clock record without nvidia-smi."""
 import json
 import os
 
@@ -17,13 +18,48 @@ def test_step_ranges_whole_graph_and_slices():
     assert not set(warm) & set(timed)  # warm-up never touches a timed slice
 
 
-def test_traffic_record_is_read_per_workload():
-    with open(os.path.join(bench.ROOT, "profiles", "match_kernel_traffic.json")) as f:
-        rec = json.load(f)
-    for wl in ("c2", "c4"):
-        assert bench.measured_traffic(wl) == rec[wl]["dram_bytes_per_launch"] > 0
-        assert "ncu" in rec[wl]["command"] and "--clock-control none" in rec[wl]["command"]
-    assert bench.measured_traffic("c1") is None
+def test_profile_record_holds_only_for_its_kernel_sources(tmp_path):
+    """An ncu record enters the roofline only when it was captured on the
+    kernel sources built here (their digest is stored with it)."""
+    path = tmp_path / "ncu.json"
+    rec = {"dram_bytes_per_launch": 1.0e6, "issue_active_pct": 30.0, "command": "ncu ..."}
+    path.write_text(json.dumps({"c13": dict(rec, kernel_sources=bench.kernel_source_digest()),
+                                "c2": dict(rec, kernel_sources="0" * 16)}))
+    assert bench.measured_profile("c13", str(path))["issue_active_pct"] == 30.0
+    assert bench.measured_profile("c2", str(path)) is None
+    assert bench.measured_profile("c4", str(path)) is None
+    committed = os.path.join(bench.ROOT, "profiles", "match_kernel_ncu.json")
+    if os.path.exists(committed):
+        for wl, r in json.load(open(committed)).items():
+            assert "ncu" in r["command"] and "--clock-control none" in r["command"], wl
+
+
+def test_reference_arm_inputs_without_the_engine(tmp_path):
+    """The reference arm writes its graph and patterns with the host-only
+    tdfs_convert tool: the same files the engine's generators give, and the
+    process that does it never loads libtdfs_b200.so."""
+    import subprocess
+    import sys
+    import tdfs_b200 as T
+    code = ("import sys, bench; E = bench.graph_via_convert('er_l', sys.argv[1]); "
+            "print(E); [print(repr(bench.convert_pattern(*s))) for s in bench.c3_pattern_specs()]; "
+            "import os; maps = open('/proc/self/maps').read(); print('libtdfs_b200' in maps, 'tdfs_b200' in sys.modules)")
+    out = subprocess.run([sys.executable, "-c", code, str(tmp_path / "g")], cwd=bench.ROOT, capture_output=True,
+                         text=True, check=True).stdout.splitlines()
+    g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
+    assert int(out[0]) == g.nedges
+    r = T.read_csr(str(tmp_path / "g"), labeled=True)
+    assert (r.colidx == g.colidx).all() and (r.labels == g.labels).all()
+    import ast
+    assert [ast.literal_eval(l) for l in out[1:9]] == [T.gen_pattern(*s) for s in bench.c3_pattern_specs()]
+    assert out[9] == "False False"
+
+
+def test_workloads_name_the_configs():
+    desc, key, pats, slices = bench.workload("c13")
+    assert key == "er_l" and slices == 1 and len(pats) == 12
+    assert [lab for _, _, lab in pats] == [False] * 4 + [True] * 8
+    assert bench.workload("c2")[3] == 1000 and bench.workload("c4")[3] == 500000
 
 
 def test_clock_record_without_nvidia_smi():
@@ -32,18 +68,11 @@ def test_clock_record_without_nvidia_smi():
     assert rec["sm_mhz"] is None and rec["reasons"] == ["nvidia-smi unavailable"]
 
 
-def test_served_stream_admission_by_estimate():
-    """The c5 stream keeps exactly the queries whose estimated count and scan
-    work fit the budget (an impossible pattern always fits, a budget of zero
-    scanned entries admits nothing that scans)."""
+def test_served_stream_queries():
+    """The config-5 stream: seeded, 3-7 vertices, labels in [0, 4), every
+    query a valid connected pattern in matching order."""
     import tdfs_b200 as T
-    g = T.gen_er(4096, 16.0, 0).set_labels(4, 2)
-    none = "v 0 9\nv 1 9\nv 2 9\ne 0 1 1\ne 0 2 1\ne 1 2 1\n"   # label 9 occurs nowhere: 0 matches, 0 scans
-    tri = "v 0 1\nv 1 1\nv 2 1\ne 0 1 1\ne 0 2 1\ne 1 2 1\n"
-    wide = "v 0 1\nv 1 1\nv 2 1\nv 3 1\ne 0 1 1\ne 1 2 1\ne 1 3 1\n"  # a labeled star: many matches
-    texts = [none, tri, wide]
-    assert bench.admit_stream(T, g, texts, 1e12, 1e12) == [0, 1, 2]
-    assert bench.admit_stream(T, g, texts, 1e12, 0) == [0]
-    est_wide = T.estimate(g, T.PatternPreprocessor(text=wide, labeled=True), 1024, 2).matches
-    assert est_wide > 0
-    assert 2 not in bench.admit_stream(T, g, texts, est_wide / 1000, 1e12)
+    a = bench.c5_queries(T.gen_pattern, 300)
+    assert a == bench.c5_queries(T.gen_pattern, 300)
+    ks = [T.PatternPreprocessor(text=t, labeled=True).nnodes for t in a]
+    assert min(ks) == 3 and max(ks) == 7
