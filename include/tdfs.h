@@ -124,6 +124,19 @@ int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
 int tdfs_count_batch_status(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
                             const tdfs_options *opt, uint64_t *counts, int *status, float *kernel_ms);
 
+/* ---- diagnostics of the last count launch on a graph (no reference
+ *      counterpart; the reference computes clock64 spans and discards them,
+ *      src/gpu_match.cu:1001,1069-1075) ---------------------------------------
+ * For a batched count over both modes, the launch of the labeled plans. */
+typedef struct {
+  uint64_t steals;       /* intra-CTA steals */
+  uint64_t splits;       /* subtree units that went through the split ring */
+  int64_t warps;         /* warps in the persistent grid */
+  double idle_fraction;  /* share of the warps' running time spent without work */
+  double mean_warp_ms;   /* mean time a warp ran, first instruction to retirement */
+} tdfs_launch_stats;
+int tdfs_last_launch(const tdfs_graph *g, tdfs_launch_stats *st);
+
 /* ---- bounded device waits, shown to run out (no reference counterpart) ----
  * Launches the match kernel over a slot that can never complete (admitted,
  * no level-0 tickets, no work held), so every warp waits for work until its

@@ -35,6 +35,7 @@ EXPORTS = [
     "tdfs_graph_open", "tdfs_graph_from_csr", "tdfs_graph_info", "tdfs_graph_free",
     "tdfs_plan_compile", "tdfs_plan_from_text", "tdfs_plan_dump", "tdfs_plan_info", "tdfs_plan_free",
     "tdfs_count", "tdfs_count_batch", "tdfs_count_batch_status", "tdfs_selftest_wait_limit",
+    "tdfs_last_launch",
     "tdfs_csr_read", "tdfs_csr_view", "tdfs_csr_write", "tdfs_csr_set_labels", "tdfs_csr_free",
     "tdfs_csr_from_arrays", "tdfs_csr_relabel", "tdfs_csr_halve",
     "tdfs_gen_er", "tdfs_gen_chung_lu", "tdfs_gen_rmat", "tdfs_gen_pattern", "tdfs_estimate",
@@ -133,6 +134,7 @@ def lib() -> C.CDLL:
     L.tdfs_count_batch_status.argtypes = [vp, C.POINTER(vp), ci, C.POINTER(Options), C.POINTER(C.c_uint64),
                                           C.POINTER(ci), C.POINTER(C.c_float)]
     L.tdfs_selftest_wait_limit.argtypes = [vp, ci, C.POINTER(C.c_float)]
+    L.tdfs_last_launch.argtypes = [vp, vp]
     L.tdfs_csr_read.argtypes = [C.c_char_p, ci, pp]
     L.tdfs_csr_view.argtypes = [vp, C.POINTER(i64), C.POINTER(i64), pp, pp, pp, C.POINTER(i32)]
     L.tdfs_csr_write.argtypes = [vp, C.c_char_p]
@@ -393,6 +395,20 @@ def selftest_wait_limit(graph: GraphPreprocessor, wait_limit_ms: int):
     ms = C.c_float()
     rc = lib().tdfs_selftest_wait_limit(graph._h, wait_limit_ms, C.byref(ms))
     return rc, ms.value
+
+
+class LaunchStats(C.Structure):
+    """tdfs_launch_stats: diagnostics of the last count launch."""
+    _fields_ = [("steals", C.c_uint64), ("splits", C.c_uint64), ("warps", C.c_int64),
+                ("idle_fraction", C.c_double), ("mean_warp_ms", C.c_double)]
+
+
+def last_launch(graph: GraphPreprocessor) -> dict:
+    """Steals, split units, grid warps, idle share and mean warp time of the
+    last count launch on this graph."""
+    st = LaunchStats()
+    _check(lib().tdfs_last_launch(graph._h, C.byref(st)))
+    return {f: getattr(st, f) for f, _ in LaunchStats._fields_}
 
 
 EDGE_CHUNK = 32  # directed edges per level-0 ticket (kEdgeChunk in match.cuh)

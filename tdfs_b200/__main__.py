@@ -1,11 +1,14 @@
-"""Command line: count a pattern on a graph file or a seeded synthetic graph.
+"""Command line: count patterns on a graph file or a seeded synthetic graph.
 
     python -m tdfs_b200 count --graph PREFIX|er:N,DEG,SEED|cl:N,M,GAMMA,CAP,SEED|rmat:SCALE,EF,SEED
-                              --pattern FILE.g|triangle|cycle4|diamond|house|k4|k5|k6|k7
-                              [--labels NLABELS,SEED] [--labeled] [--reps R]
+                              --pattern FILE.g|triangle|cycle4|diamond|house|k4|k5|k6|k7|gen:K,DENSITY,NLABELS,SEED
+                              [--pattern ...] [--labels NLABELS,SEED] [--labeled] [--reps R]
                               [--edges BEGIN,END] [--opt name=value ...]
 
-Prints one line per repetition: pattern, kernel ms, count (the ulb/lb line).
+With one pattern, prints one line per repetition: pattern, kernel ms, count
+(the ulb/lb line).  With several, they run as one batched launch
+(tdfs_count_batch) and each repetition prints "batch", the kernel ms and the
+counts.  `gen:` patterns come from tdfs_gen_pattern.
 """
 from __future__ import annotations
 
@@ -47,7 +50,7 @@ def main(argv=None):
     sub = ap.add_subparsers(dest="cmd", required=True)
     c = sub.add_parser("count")
     c.add_argument("--graph", required=True)
-    c.add_argument("--pattern", required=True)
+    c.add_argument("--pattern", required=True, action="append")
     c.add_argument("--labels")
     c.add_argument("--labeled", action="store_true")
     c.add_argument("--reps", type=int, default=1)
@@ -55,10 +58,16 @@ def main(argv=None):
     c.add_argument("--opt", action="append", default=[])
     args = ap.parse_args(argv)
     g = load_graph(args.graph, args.labels, args.labeled)
-    if args.pattern in NAMED:
-        p = T.PatternPreprocessor(text=NAMED[args.pattern], labeled=args.labeled)
-    else:
-        p = T.PatternPreprocessor(args.pattern, labeled=args.labeled)
+    plans = []
+    for spec in args.pattern:
+        if spec in NAMED:
+            plans.append(T.PatternPreprocessor(text=NAMED[spec], labeled=args.labeled))
+        elif spec.startswith("gen:"):
+            k, d, nl, seed = spec[4:].split(",")
+            plans.append(T.PatternPreprocessor(text=T.gen_pattern(int(k), float(d), int(nl), int(seed)),
+                                               labeled=args.labeled))
+        else:
+            plans.append(T.PatternPreprocessor(spec, labeled=args.labeled))
     kw = {}
     for o in args.opt:
         k, v = o.split("=")
@@ -68,8 +77,12 @@ def main(argv=None):
         kw["edge_begin"], kw["edge_end"] = int(b), int(e)
     opt = T.default_options(**kw)
     for _ in range(args.reps):
-        r = T.count(g, p, opt)
-        print(f"{args.pattern}\t{r.kernel_ms:f}\t{r.count}", flush=True)
+        if len(plans) == 1:
+            r = T.count(g, plans[0], opt)
+            print(f"{args.pattern[0]}\t{r.kernel_ms:f}\t{r.count}", flush=True)
+        else:
+            counts, ms = T.count_batch(g, plans, opt)
+            print("batch\t%f\t%s" % (ms, " ".join(str(c) for c in counts)), flush=True)
     return 0
 
 

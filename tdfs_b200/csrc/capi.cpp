@@ -291,6 +291,7 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
     if (in.ntickets == 0) ++h->ctl.completed;
     h->plan[i] = *plans[i];
   }
+  g->last_warps = (int64_t)s.blocks * s.warps_per_block;
   if (o.graph_capture) return run_captured(g, s, labeled, n, ms, raw, status);
   cudaStream_t st = static_cast<cudaStream_t>(o.stream);
   SlotTable *d = g->tab;
@@ -308,10 +309,9 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   if (ms) cudaEventRecord(ev0, st);
   rc = launch_match(labeled, graph_view(g), g->ctl, d, g->queue, queue_hdr(g), s.cfg, s.blocks, s.warps_per_block, st);
   if (ms) cudaEventRecord(ev1, st);
-  RunCtl hc;
   if (!rc) {
     e = cudaMemcpyAsync(h->hot, d->hot, sizeof(SlotHot) * n, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, g->ctl, sizeof hc, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(g->hctl, g->ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_err(e, "match kernel");
   }
@@ -322,7 +322,7 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (rc) return rc;
-  return collect(hc, h->hot, n, raw, status);
+  return collect(*g->hctl, h->hot, n, raw, status);
 }
 
 }  // namespace
@@ -519,7 +519,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
   };
   const std::vector<Knob> knobs = {
       {&tdfs_options::warps_per_block, {4, 8}},
-      {&tdfs_options::chunk_cap, {128, 256, 512, 1024}},
+      {&tdfs_options::chunk_cap, {64, 128, 256, 512, 1024}},
       {&tdfs_options::merge_window, {-1, 128, 256}},
       {&tdfs_options::merge_ratio, {1, 4, 16}},
       // (stealing stays on: without it one warp keeps a hub's whole subtree,
@@ -601,6 +601,19 @@ int tdfs_selftest_wait_limit(tdfs_graph *g, int wait_limit_ms, float *kernel_ms)
   cudaEventDestroy(ev1);
   if (rc) return rc;
   if (hc.error) return fail(hc.error, "the launch reported device status %d after its bounded waits", hc.error);
+  return TDFS_OK;
+}
+
+int tdfs_last_launch(const tdfs_graph *g, tdfs_launch_stats *st) {
+  if (!g || !st) return fail(TDFS_ERR_ARG, "null argument");
+  std::memset(st, 0, sizeof *st);
+  if (!g->hctl || !g->last_warps) return fail(TDFS_ERR_ARG, "no launch on this graph yet");
+  const RunCtl &c = *g->hctl;
+  st->steals = c.steals;
+  st->splits = c.splits;
+  st->warps = g->last_warps;
+  st->idle_fraction = c.warp_ns ? (double)c.idle_ns / (double)c.warp_ns : 0.0;
+  st->mean_warp_ms = (double)c.warp_ns / 1e6 / (double)g->last_warps;
   return TDFS_OK;
 }
 

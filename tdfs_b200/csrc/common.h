@@ -58,7 +58,10 @@ struct alignas(128) RunCtl {
   unsigned long long steals;     // diagnostics: intra-block steals
   unsigned long long splits;     // diagnostics: units through the global queue
   int32_t error;                 // TDFS_ERR_* raised by the kernel
-  char pad1_[108];
+  int32_t pad_;
+  unsigned long long idle_ns;    // diagnostics: summed time warps spent without work
+  unsigned long long warp_ns;    // diagnostics: summed time warps ran
+  char pad1_[88];
 };
 
 // Error reporting shared by the C ABI implementation files.

@@ -129,6 +129,7 @@ struct tdfs_graph {
   tdfs::RunCtl *hctl;
   void *graphs;           // cache of instantiated launch graphs (capi.cpp)
   size_t bytes;
+  int64_t last_warps;     // warps in the grid of the last count launch (diagnostics)
 };
 
 namespace tdfs {

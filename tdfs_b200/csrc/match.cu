@@ -1105,6 +1105,7 @@ struct Engine {
   // tickets of an open slot, a steal from its CTA, or a unit from the ring).
   __device__ void run(int nwarps, int me) {
     int level = 0, base = 1;
+    if (lane == 0) t_start = now_ns();
     bool hungry = false;  // counted in ctl->hungry (warps polling for work)
     bool holding = false;
     unsigned claims = 0;
@@ -1147,6 +1148,10 @@ struct Engine {
           if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
           hungry = false;
           idle_since = 0;
+          if (lane == 0 && idle_start) {
+            idle_total += now_ns() - idle_start;
+            idle_start = 0;
+          }
           nap = 256;
           continue;
         }
@@ -1234,6 +1239,12 @@ struct Engine {
       --level;
     }
     if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
+    if (lane == 0) {
+      const unsigned long long t = now_ns();
+      if (idle_start) idle_total += t - idle_start;
+      atomicAdd(&ctl->idle_ns, idle_total);
+      atomicAdd(&ctl->warp_ns, t - t_start);
+    }
     __syncwarp();
   }
 
@@ -1243,11 +1254,13 @@ struct Engine {
   // a timeout; a serving launch simply retires and the host relaunches it.
   unsigned nap = 256;
   unsigned long long idle_since = 0;
+  unsigned long long idle_start = 0, idle_total = 0, t_start = 0;  // diagnostics (lane 0)
   __device__ bool wait_for_work() {
     int ok = 1;
     if (lane == 0) {
       const unsigned long long t = now_ns();
       if (!idle_since) idle_since = t;
+      if (!idle_start) idle_start = t;
       const SlotCtl &C = tab->ctl;
       const int shut = *(volatile int32_t *)&C.shutdown;
       // serving: the idle clock runs only while every admitted query is
@@ -1296,6 +1309,8 @@ __global__ void init_kernel(RunCtl *ctl, QueueHdr *qh) {
     ctl->hungry = 0;
     ctl->steals = 0;
     ctl->splits = 0;
+    ctl->idle_ns = 0;
+    ctl->warp_ns = 0;
     ctl->error = 0;
     qh->head = 0;
     qh->tail = 0;
