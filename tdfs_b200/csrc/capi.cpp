@@ -29,7 +29,10 @@ namespace tdfs {
 
 namespace {
 
+// Report a failed CUDA call and clear the runtime's last-error slot, so the
+// error cannot resurface in a later launch check.
 int cuda_err(cudaError_t e, const char *what) {
+  (void)cudaGetLastError();
   return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
@@ -171,12 +174,14 @@ int enqueue_launch(tdfs_graph *g, const LaunchShape &s, bool labeled, int n, cud
   if (e == cudaSuccess) e = cudaMemcpyAsync(d->plan, h->plan, sizeof(DevPlan) * n, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_err(e, "slot table upload");
   init_launch(g->ctl, queue_hdr(g), st);
-  e = cudaEventRecord(k0, st);
+  // external records: captured as event-record nodes, so they time the
+  // kernel when the graph replays (a plain record is only a join point)
+  e = cudaEventRecordWithFlags(k0, st, cudaEventRecordExternal);
   if (e != cudaSuccess) return cuda_err(e, "kernel start event");
   int rc = launch_match(labeled, graph_view(g), g->ctl, d, g->queue, queue_hdr(g), s.cfg, s.blocks,
                         s.warps_per_block, st);
   if (rc) return rc;
-  e = cudaEventRecord(k1, st);
+  e = cudaEventRecordWithFlags(k1, st, cudaEventRecordExternal);
   if (e != cudaSuccess) return cuda_err(e, "kernel end event");
   e = cudaMemcpyAsync(h->hot, d->hot, sizeof(SlotHot) * n, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(g->hctl, g->ctl, sizeof(RunCtl), cudaMemcpyDeviceToHost, st);

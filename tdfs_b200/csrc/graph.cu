@@ -61,7 +61,10 @@ __global__ void narrow_labels_kernel(const int32_t *__restrict__ in, int32_t n, 
   }
 }
 
+// Report a failed CUDA call and clear the runtime's last-error slot, so the
+// error cannot resurface in a later launch check.
 int cuda_fail(cudaError_t e, const char *what) {
+  (void)cudaGetLastError();
   return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
@@ -72,6 +75,7 @@ int cuda_fail(cudaError_t e, const char *what) {
 // labels.  *bad becomes nonzero when a label lies outside [0, 254].
 int prepare_graph_arrays(const int64_t *rowptr, const int32_t *colidx, int32_t n, const int32_t *labels,
                          int32_t *src, int32_t *maxnd, uint8_t *label8, int32_t *bad, cudaStream_t st) {
+  (void)cudaGetLastError();  // the check below must see these launches' errors only
   if (n > 0) {
     const int threads = 256;
     const int64_t want = ((int64_t)n * 32 + threads - 1) / threads;
@@ -222,6 +226,7 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
     e = cudaMemcpyAsync(g->label, lab8.data(), (size_t)n, cudaMemcpyHostToDevice, st);
   int rc = TDFS_OK;
   if (e == cudaSuccess && n > 0) {
+    (void)cudaGetLastError();  // the check below must see these launches' errors only
     const int threads = 256;
     const int64_t want = ((int64_t)n * 32 + threads - 1) / threads;
     const int blocks = (int)std::min<int64_t>(want, 148 * 16);

@@ -12,6 +12,7 @@
 
 #include <climits>
 #include <cstdio>
+#include <mutex>
 
 #include "match.cuh"
 
@@ -1328,9 +1329,27 @@ size_t warp_smem_bytes(int k, int cap, int window, bool fixed) {
 
 namespace {
 
+// The dynamic shared-memory limit of each kernel instance only ever grows:
+// setting it lower for a small launch would make a later, larger launch of
+// the same instance fail with an invalid argument.  Tracked per device and
+// instance, raised under a lock.
+template <bool LAB, int MINB>
+cudaError_t ensure_dynamic_smem(size_t smem) {
+  static std::mutex mu;
+  static size_t set_to[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= 64) return e != cudaSuccess ? e : cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(mu);
+  if (smem <= set_to[dev]) return cudaSuccess;
+  e = cudaFuncSetAttribute(match_kernel<LAB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) set_to[dev] = smem;
+  return e;
+}
+
 template <bool LAB, int MINB>
 cudaError_t occupancy(int *n, int warps_per_block, size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(match_kernel<LAB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = ensure_dynamic_smem<LAB, MINB>(smem);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(n, match_kernel<LAB, MINB>, warps_per_block * 32, smem);
   return e;
 }
@@ -1355,6 +1374,13 @@ int launch_match(bool labeled, const DevGraph &g, RunCtl *ctl, SlotTable *tab, S
                  const KernelCfg &cfg, int blocks, int warps_per_block, cudaStream_t stream) {
   const size_t smem = (size_t)cfg.warp_bytes * warps_per_block;
   const dim3 grid(blocks), block(warps_per_block * 32);
+  cudaError_t a;
+  if (labeled)
+    a = cfg.wide_regs ? ensure_dynamic_smem<true, 3>(smem) : ensure_dynamic_smem<true, 4>(smem);
+  else
+    a = cfg.wide_regs ? ensure_dynamic_smem<false, 3>(smem) : ensure_dynamic_smem<false, 4>(smem);
+  if (a != cudaSuccess) return fail(TDFS_ERR_CUDA, "match kernel shared memory: %s", cudaGetErrorString(a));
+  (void)cudaGetLastError();  // the check below must see this launch's error only
   if (labeled) {
     if (cfg.wide_regs) match_kernel<true, 3><<<grid, block, smem, stream>>>(g, cfg, ctl, tab, units, qh);
     else match_kernel<true, 4><<<grid, block, smem, stream>>>(g, cfg, ctl, tab, units, qh);

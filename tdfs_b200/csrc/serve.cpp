@@ -109,7 +109,10 @@ struct Server {
 
 namespace {
 
-int cuda_err(cudaError_t e, const char *what) { return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e)); }
+int cuda_err(cudaError_t e, const char *what) {
+  (void)cudaGetLastError();  // a reported error must not resurface in a later launch check
+  return fail(TDFS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
 
 // Open a fresh slot table (no kernel may be running on it).
 int open_epoch(Server &S) {

@@ -62,6 +62,13 @@ std::mutex g_setup_mu;
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+// Report a failed CUDA call (what: "<call>: %s") and clear the runtime's
+// last-error slot, so the error cannot resurface in a later launch check.
+int cuda_fail_static(const char *what, cudaError_t e) {
+  (void)cudaGetLastError();
+  return fail(TDFS_ERR_CUDA, what, cudaGetErrorString(e));
+}
+
 // Fixed layout of the array (offsets in bytes).
 struct Layout {
   size_t ctl, bad, units, qhdr, tab, src, maxnd, label, end;
@@ -103,14 +110,14 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
                 "graph needs %zu bytes of scratch (n=%lld, E=%lld); the fixed array holds %zu bytes", L.end,
                 (long long)n, (long long)nedges, kScratchBytes);
   cudaError_t e = cudaSetDevice(device);
-  if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return cuda_fail_static("cudaSetDevice: %s", e);
   unsigned char *base;
   {
     std::lock_guard<std::mutex> lk(g_setup_mu);
     if (!g_scratch_addr[device]) {
       void *addr = nullptr;
       e = cudaGetSymbolAddress(&addr, g_scratch);
-      if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+      if (e != cudaSuccess) return cuda_fail_static("cudaGetSymbolAddress: %s", e);
       g_scratch_addr[device] = static_cast<unsigned char *>(addr);
     }
     base = g_scratch_addr[device];
@@ -121,7 +128,7 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     e = cudaStreamIsCapturing(st, &cs);
-    if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "cudaStreamIsCapturing: %s", cudaGetErrorString(e));
+    if (e != cudaSuccess) return cuda_fail_static("cudaStreamIsCapturing: %s", e);
     if (cs != cudaStreamCaptureStatusNone)
       return fail(TDFS_ERR_ARG, "tdfs_count_static cannot be called on a stream that is being captured");
   }
@@ -138,7 +145,7 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   // derived graph arrays, written into the scratch (each call recomputes them)
   int32_t *bad = reinterpret_cast<int32_t *>(base + L.bad);
   e = cudaMemsetAsync(bad, 0, sizeof(int32_t), st);
-  if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "scratch clear: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return cuda_fail_static("scratch clear: %s", e);
   int rc = prepare_graph_arrays(d_rowptr, d_colidx, (int32_t)n, plan.labeled ? d_labels : nullptr, src, maxnd,
                                 label8, bad, st);
   if (rc) return rc;
@@ -186,7 +193,7 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   if (e == cudaSuccess) e = cudaMemcpyAsync(&tab->hot[0], &h_hot, sizeof h_hot, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&tab->info[0], &h_info, sizeof h_info, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&tab->plan[0], &plan, sizeof plan, cudaMemcpyHostToDevice, st);
-  if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "slot upload: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return cuda_fail_static("slot upload: %s", e);
   init_launch(ctl, qh, st);  // clears the control block and the split ring
   rc = launch_match(plan.labeled != 0, g, ctl, tab, units, qh, s.cfg, s.blocks, s.warps_per_block, st);
   if (rc) return rc;
@@ -195,7 +202,7 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_bad, bad, sizeof h_bad, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h_run, ctl, sizeof h_run, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) return fail(TDFS_ERR_CUDA, "match kernel: %s", cudaGetErrorString(e));
+  if (e != cudaSuccess) return cuda_fail_static("match kernel: %s", e);
   if (h_bad) return fail(TDFS_ERR_FORMAT, "vertex labels must lie in [0, 254]");
   if (h_run.error) return fail(h_run.error, "device error %d", h_run.error);
   if (h_hot.state != kSlotDone) return fail(TDFS_ERR_TIMEOUT, "the query did not complete");
