@@ -74,6 +74,9 @@ typedef struct {
                            TDFS_ERR_TIMEOUT; the others complete normally */
   int wait_limit_ms;    /* bound on a warp's idle wait for work before the launch reports
                            TDFS_ERR_TIMEOUT (0 auto = 30000) */
+  int split_rush_us;    /* once a quarter of the grid's warps are idle (the tail of a launch),
+                           subtrees may be split after this many microseconds instead of
+                           split_after_us (0 auto = 10, -1 off) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

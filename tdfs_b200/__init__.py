@@ -73,6 +73,7 @@ class Options(C.Structure):
         ("lane_list", C.c_int),
         ("work_budget", C.c_int64),
         ("wait_limit_ms", C.c_int),
+        ("split_rush_us", C.c_int),
     ]
 
 

@@ -117,6 +117,14 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   const int per_sm = o.blocks_per_sm > 0 ? std::min(o.blocks_per_sm, fit) : fit;
   c.wide_regs = per_sm <= fit_wide ? 1 : 0;
   s.blocks = prop.multiProcessorCount * per_sm;
+  // the tail rush: once a quarter of the grid is idle, split after rush_us
+  if (o.split_rush_us < 0 || c.split_after_ns == 0) {
+    c.rush_hungry = 0;
+  } else {
+    c.rush_hungry = std::max(1, s.blocks * s.warps_per_block / 4);
+    c.rush_ns = (o.split_rush_us > 0 ? o.split_rush_us : 10) * 1000;
+    if (c.rush_ns > c.split_after_ns) c.rush_ns = c.split_after_ns;
+  }
   *out = s;
   return TDFS_OK;
 }
@@ -536,6 +544,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::edge_chunk, {1, 4, 8, 32}},
       {&tdfs_options::fixed_stage, {-1, 1}},
       {&tdfs_options::split_after_us, {-1, 5, 50, 150, 500}},
+      {&tdfs_options::split_rush_us, {-1, 2, 10, 40}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {

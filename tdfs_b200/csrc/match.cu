@@ -849,6 +849,17 @@ struct Engine {
     __syncwarp();
   }
 
+  // How long a warp's base subtree must have run before others may split it:
+  // cfg.split_after_ns normally (small subtrees finish where they started),
+  // cfg.rush_ns once at least cfg.rush_hungry warps of the grid are idle --
+  // the tail of a launch, where a few large subtrees hold all the work left
+  // and every split is worth more than it costs.
+  __device__ __forceinline__ unsigned long long split_gate() {
+    if (cfg.rush_hungry > 0 && *(volatile int32_t *)&ctl->hungry >= cfg.rush_hungry)
+      return (unsigned long long)cfg.rush_ns;
+    return (unsigned long long)cfg.split_after_ns;
+  }
+
   // Steal half of the remaining items at the shallowest level of another
   // warp of this CTA.  The thief copies the victim's plan, prefix and the
   // upper half of its items, takes a hold on the victim's slot, then CASes
@@ -861,8 +872,8 @@ struct Engine {
     // the largest one on ties
     unsigned long long key = 0;
     const unsigned long long now = now_ns();
-    if (lane < nwarps && lane != me &&
-        now - *(volatile const unsigned long long *)&warp_at(lane).t_base >= (unsigned long long)cfg.split_after_ns) {
+    const unsigned long long gate = split_gate();
+    if (lane < nwarps && lane != me && now - *(volatile const unsigned long long *)&warp_at(lane).t_base >= gate) {
       const WarpSmem &V = warp_at(lane);
       for (int l = 1; l <= kMaxK - 2; ++l) {
         const unsigned long long w = *(volatile const unsigned long long *)&V.word[l];
@@ -1028,8 +1039,7 @@ struct Engine {
   // shallowest remaining items into the global ring.
   __device__ void maybe_donate(int level) {
     int hungry = 0;
-    if (lane == 0 && now_ns() - W.t_base >= 4ull * (unsigned long long)cfg.split_after_ns)
-      hungry = *(volatile int32_t *)&ctl->hungry;
+    if (lane == 0 && now_ns() - W.t_base >= 4ull * split_gate()) hungry = *(volatile int32_t *)&ctl->hungry;
     hungry = __shfl_sync(kFull, hungry, 0);
     if (hungry <= 0) return;
     if (lane == 0) {

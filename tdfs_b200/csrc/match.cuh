@@ -60,6 +60,8 @@ struct KernelCfg {
   int32_t lane_list;    // last level: siblings' lists up to max(lane_list, 4 |F|) long go to the
                         // flattened batch pass (0 = off: one warp pass per sibling)
   int32_t budgeted;     // 1: some slot has a work budget (SlotInfo::budget); warps account their work
+  int32_t rush_hungry;  // with at least this many warps idle (0 = never) ...
+  int32_t rush_ns;      // ... subtrees may be split after this long instead of split_after_ns
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)

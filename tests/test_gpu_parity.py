@@ -30,8 +30,10 @@ OPTION_SETS = [
     {"fixed_stage": -1, "edge_chunk": 32, "steal_min": 8},  # no last-level staging
     {"edge_chunk": 1, "steal_first": 2, "split_after_us": -1},  # one edge per ticket, eager splits
     {"edge_chunk": 4, "blocks_per_sm": 2, "steal_first": 32},
-    {"lane_list": 64, "chunk_cap": 128},   # most last-level parents counted one per lane
-    {"lane_list": -1},                     # one warp-wide pass per last-level parent
+    {"lane_list": 64, "chunk_cap": 128},   # longer lists in the flattened last-level pass
+    {"lane_list": -1},                     # one warp-wide pass per last-level sibling
+    {"split_rush_us": -1, "steal_first": 2},            # no tail rush
+    {"split_rush_us": 1, "split_after_us": 400, "fixed_stage": -1},  # long gate, 1 us in the tail
 ]
 
 
