@@ -201,7 +201,7 @@ int tdfs_server_destroy(tdfs_server *s); /* drains admitted queries, stops the k
  * int32, needed for a labeled pattern) and every working buffer lives in one fixed 48 MiB array inside the
  * library's device image, held on each GPU that uses the library until the
  * process exits.  Graphs whose derived arrays do not fit in it are rejected
- * with TDFS_ERR_CAPACITY (about 4*E + 5*n bytes, up to ~30 MiB, must fit).
+ * with TDFS_ERR_CAPACITY (about 4*E + 5*n bytes, up to ~28 MiB, must fit).
  * d_colidx must be 16-byte aligned (TDFS_ERR_ARG otherwise): the kernel reads
  * adjacency windows with 16-byte loads.  When E is not a multiple of 4 those
  * windows are turned off, so nothing past colidx[E-1] is read.  The first

@@ -45,9 +45,11 @@ constexpr int kMaxSlots = 16384;
 
 enum : int32_t { kSlotEmpty = 0, kSlotActive = 1, kSlotDone = 2 };
 
-// Counters that warps update: one 128-byte line per slot.
+// Counters that warps update: the ticket counter, the hottest (one atomic
+// per level-0 ticket), on a 128-byte line of its own; the rest on a second.
 struct alignas(128) SlotHot {
   unsigned long long ticket;  // next level-0 chunk ticket
+  char pad_ticket_[120];
   unsigned long long count;   // raw count (before the |Aut| multiplier)
   int32_t holders;            // warps holding this query's work + its queued units
   int32_t state;              // kSlotActive -> kSlotDone (by the completing warp)

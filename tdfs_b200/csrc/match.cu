@@ -815,6 +815,26 @@ struct Engine {
     }
   }
 
+  // A warp that holds slot W.slot and has finished its subtree keeps the hold
+  // and takes the slot's next level-0 ticket directly: one atomic per ticket
+  // instead of a release, a new hold and a take on the slot's lines.  Returns
+  // false when the slot has no tickets left; the hold is then dropped (and
+  // the count flushed).
+  __device__ bool next_ticket_same_slot() {
+    const int s = W.slot;
+    for (;;) {
+      long long t = -1;
+      if (lane == 0) {
+        const unsigned long long tk = atomicAdd(&tab->hot[s].ticket, 1ull);
+        t = (long long)tk < __ldcg(&tab->info[s].ntickets) ? (long long)tk : -1;
+        if (t < 0) release_lane0(s);
+      }
+      t = __shfl_sync(kFull, t, 0);
+      if (t < 0) return false;
+      if (fetch_chunk(s, t)) return true;
+    }
+  }
+
   // New batch of `n` items at level l (1 = edge pairs, >= 2 candidates).
   __device__ __forceinline__ void publish(int l, int n) {
     const unsigned long long gen = (W.word[l] >> 32) + 1;
@@ -1130,14 +1150,15 @@ struct Engine {
     __syncwarp();
     for (;;) {
       if (level < base) {
-        // ---- release the finished subtree, then acquire new work ----
-        if (holding) {
-          if (lane == 0) release_lane0(W.slot);
-          __syncwarp();
-          holding = false;
-        }
+        // ---- the finished subtree: the next ticket of the same slot, else
+        // release and acquire new work ----
         level = 0;
-        if (take_tickets()) level = base = 1;
+        if (holding) {
+          holding = false;
+          if (next_ticket_same_slot()) level = base = 1;
+          __syncwarp();
+        }
+        if (!level && take_tickets()) level = base = 1;
         if (!level && cfg.steal) {
           // largest grains first: a big share of a CTA neighbour's level, a
           // split unit from the ring (work of other SMs), then any remainder
