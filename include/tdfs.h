@@ -77,6 +77,11 @@ typedef struct {
   int split_rush_us;    /* once a quarter of the grid's warps are idle (the tail of a launch),
                            subtrees may be split after this many microseconds instead of
                            split_after_us (0 auto = 10, -1 off) */
+  int leaf_steal_min;   /* items of the last stored level (each only counts leaves) are stolen or
+                           donated only while at least this many are left (0 auto = 64, -1 = 2) */
+  int label_index;      /* labeled plans take level-0 tickets over the graph's label index: only
+                           the edges whose end labels match the plan's first two vertices
+                           (0 auto = on, -1 off: every edge id, filtered) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

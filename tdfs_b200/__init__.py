@@ -74,6 +74,8 @@ class Options(C.Structure):
         ("work_budget", C.c_int64),
         ("wait_limit_ms", C.c_int),
         ("split_rush_us", C.c_int),
+        ("leaf_steal_min", C.c_int),
+        ("label_index", C.c_int),
     ]
 
 

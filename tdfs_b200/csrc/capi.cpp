@@ -79,6 +79,7 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.budgeted = o.work_budget > 0 ? 1 : 0;
   c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
   c.steal_first = o.steal_first > 0 ? o.steal_first : 8;
+  c.leaf_min = o.leaf_steal_min > 0 ? o.leaf_steal_min : (o.leaf_steal_min < 0 ? 2 : 64);
   c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 32);
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
@@ -127,6 +128,21 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   }
   *out = s;
   return TDFS_OK;
+}
+
+// The level-0 range of a slot: the edge ids [eb, ee), or -- for a labeled
+// plan on a graph with a label index -- the positions of the index group of
+// the plan's first two labels that hold those ids.
+void level0_range(const tdfs_graph *g, const DevPlan &p, int64_t eb, int64_t ee, bool use_index, SlotInfo *in) {
+  ee = std::max(eb, ee);
+  in->perm = 0;
+  if (use_index && p.labeled && g->lindex) {
+    label_range(*g->lindex, p.label[0], p.label[1], eb, ee, &in->e_begin, &in->e_end);
+    in->perm = 1;
+    return;
+  }
+  in->e_begin = eb;
+  in->e_end = ee;
 }
 
 namespace {
@@ -289,15 +305,14 @@ int run_batch(tdfs_graph *g, const DevPlan *const *plans, int n, const tdfs_opti
   std::memset(&h->ctl, 0, sizeof h->ctl);
   h->ctl.admitted = (unsigned long long)n;
   h->ctl.shutdown = 1;
-  const int chunk = auto_chunk(std::max<int64_t>(0, ee - eb), stride, s.blocks * s.warps_per_block, o.edge_chunk);
+  const int warps = s.blocks * s.warps_per_block;
   for (int i = 0; i < n; ++i) {
     SlotInfo &in = h->info[i];
-    in.e_begin = eb;
-    in.e_end = std::max(eb, ee);
+    level0_range(g, *plans[i], eb, ee, o.label_index >= 0, &in);
     in.stride = stride;
     in.phase = o.edge_phase;
-    in.chunk = chunk;
-    in.ntickets = ticket_count(in.e_begin, in.e_end, stride, o.edge_phase, chunk);
+    in.chunk = auto_chunk(in.e_end - in.e_begin, stride, warps, o.edge_chunk);
+    in.ntickets = ticket_count(in.e_begin, in.e_end, stride, o.edge_phase, in.chunk);
     in.budget = o.work_budget;
     std::memset(&h->hot[i], 0, sizeof h->hot[i]);
     h->hot[i].state = in.ntickets > 0 ? kSlotActive : kSlotDone;  // an empty range is done at once
@@ -545,6 +560,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::fixed_stage, {-1, 1}},
       {&tdfs_options::split_after_us, {-1, 5, 50, 150, 500}},
       {&tdfs_options::split_rush_us, {-1, 2, 10, 40}},
+      {&tdfs_options::leaf_steal_min, {-1, 16, 64, 256}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {

@@ -44,6 +44,7 @@ struct DevGraph {
   const int32_t *src;      // edge -> source vertex, nedges
   const uint8_t *label;    // n, or nullptr
   const int32_t *maxnd;    // max degree over each vertex's neighbours
+  const int32_t *lperm;    // level-0 label index (labeled graphs), or nullptr
   int64_t nedges;
   int32_t n;
   int32_t max_degree;

@@ -14,7 +14,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -184,12 +186,30 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
     return fail(TDFS_ERR_CUDA, "no CUDA device visible (the tdfs engine has no CPU path)");
   if (device < 0 || device >= ndev) return fail(TDFS_ERR_ARG, "device %d out of range", device);
   std::vector<uint8_t> lab8;
+  std::unique_ptr<LabelIndex> lindex;
   if (labels) {
     lab8.resize((size_t)n);
     for (int64_t i = 0; i < n; ++i) {
       if (labels[i] < 0 || labels[i] > 254)
         return fail(TDFS_ERR_FORMAT, "vertex labels must lie in [0, 254] for the device label array");
       lab8[(size_t)i] = (uint8_t)labels[i];
+    }
+    // level-0 label index: a stable counting sort of the edge ids by
+    // (label(src), label(dst))
+    lindex.reset(new LabelIndex);
+    std::vector<int64_t> &off = lindex->off;
+    off.assign(65537, 0);
+    for (int64_t v = 0; v < n; ++v) {
+      const int ls = lab8[(size_t)v] << 8;
+      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) ++off[(size_t)(ls | lab8[(size_t)colidx[j]]) + 1];
+    }
+    for (size_t k = 1; k < off.size(); ++k) off[k] += off[k - 1];
+    std::vector<int64_t> at(off.begin(), off.end() - 1);
+    lindex->perm.resize((size_t)nedges);
+    for (int64_t v = 0; v < n; ++v) {
+      const int ls = lab8[(size_t)v] << 8;
+      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j)
+        lindex->perm[(size_t)at[(size_t)(ls | lab8[(size_t)colidx[j]])]++] = (int32_t)j;
     }
   }
   cudaError_t e = cudaSetDevice(device);
@@ -199,7 +219,8 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   const size_t o_src = o_col + align256(sizeof(int32_t) * (size_t)(nedges + kColPad));
   const size_t o_maxnd = o_src + align256(sizeof(int32_t) * (size_t)(nedges ? nedges : 1));
   const size_t o_label = o_maxnd + align256(sizeof(int32_t) * (size_t)(n ? n : 1));
-  const size_t total = o_label + align256((size_t)(labels && n ? n : 1));
+  const size_t o_perm = o_label + align256((size_t)(labels && n ? n : 1));
+  const size_t total = o_perm + align256(sizeof(int32_t) * (size_t)(labels && nedges ? nedges : 1));
   char *base = nullptr;
   e = cudaMalloc(&base, total);
   if (e != cudaSuccess) return cuda_fail(e, "graph arrays");
@@ -216,6 +237,7 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   g->src = reinterpret_cast<int32_t *>(base + o_src);
   g->maxnd = reinterpret_cast<int32_t *>(base + o_maxnd);
   g->label = labels ? reinterpret_cast<uint8_t *>(base + o_label) : nullptr;
+  g->lperm = labels ? reinterpret_cast<int32_t *>(base + o_perm) : nullptr;
   g->bytes = total;
   const cudaStream_t st = cudaStreamPerThread;
   e = cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st);
@@ -224,6 +246,8 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   if (e == cudaSuccess) e = cudaMemsetAsync(g->colidx + nedges, 0x7f, sizeof(int32_t) * kColPad, st);
   if (e == cudaSuccess && labels && n)
     e = cudaMemcpyAsync(g->label, lab8.data(), (size_t)n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && labels && nedges)
+    e = cudaMemcpyAsync(g->lperm, lindex->perm.data(), sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
   int rc = TDFS_OK;
   if (e == cudaSuccess && n > 0) {
     (void)cudaGetLastError();  // the check below must see these launches' errors only
@@ -242,8 +266,20 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
     delete g;
     return rc;
   }
+  g->lindex = lindex.release();
   *out = g;
   return TDFS_OK;
+}
+
+void label_range(const LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e) {
+  *b = *e = 0;
+  if (l0 < 0 || l0 > 254 || l1 < 0 || l1 > 254) return;  // a label no vertex has: nothing to do
+  const size_t key = (size_t)(l0 << 8 | l1);
+  const int32_t *g0 = x.perm.data() + x.off[key], *g1 = x.perm.data() + x.off[key + 1];
+  // ids ascend within a group: the edge-id range is a position range
+  *b = x.off[key] + (std::lower_bound(g0, g1, (int32_t)std::min<int64_t>(eb, INT32_MAX)) - g0);
+  *e = x.off[key] + (std::lower_bound(g0, g1, (int32_t)std::min<int64_t>(ee, INT32_MAX)) - g0);
+  if (ee > INT32_MAX) *e = x.off[key + 1];
 }
 
 void graph_release(tdfs_graph *g) {
@@ -254,6 +290,7 @@ void graph_release(tdfs_graph *g) {
   release_graphs(g);
   release_workspace(g);
   cudaFree(g->arrays);
+  delete g->lindex;
   cudaSetDevice(cur);
   delete g;
 }
@@ -265,6 +302,7 @@ DevGraph graph_view(const tdfs_graph *g) {
   v.src = g->src;
   v.label = g->label;
   v.maxnd = g->maxnd;
+  v.lperm = g->lperm;
   v.nedges = g->nedges;
   v.n = (int32_t)g->n;
   v.max_degree = g->max_degree;

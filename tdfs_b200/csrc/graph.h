@@ -5,6 +5,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.h"
 
 namespace tdfs {
@@ -61,12 +63,12 @@ struct alignas(128) SlotHot {
 
 // Written by the host at admission, read-only for the kernel.
 struct SlotInfo {
-  int64_t e_begin;   // level-0 edge range and round-robin dealing
-  int64_t e_end;
+  int64_t e_begin;   // level-0 edge range and round-robin dealing (positions in the
+  int64_t e_end;     //   label index when `perm` is set, else edge ids)
   int64_t ntickets;  // tickets of this slot
   int32_t stride, phase;
   int32_t chunk;     // directed edges per ticket (1, 2, 4, ..., 32)
-  int32_t pad_;
+  int32_t perm;      // 1: level-0 positions index DevGraph::lperm (labeled plans)
   int64_t budget;    // work units this query may spend (0 = unlimited)
 };
 
@@ -111,6 +113,22 @@ struct Workspace {
 
 }  // namespace tdfs
 
+namespace tdfs {
+
+// Level-0 label index of a labeled graph: every directed edge id, grouped by
+// the label pair (label(src), label(dst)) and in ascending id within a group.
+// A labeled plan's level-0 tickets run over its group only, so none of them is
+// spent on edges the label test would drop.
+struct LabelIndex {
+  std::vector<int32_t> perm;  // host copy of the device array
+  std::vector<int64_t> off;   // group of key = 256 * l0 + l1 is perm[off[key], off[key + 1])
+};
+
+// Group range of plan labels (l0, l1) restricted to edge ids [eb, ee).
+void label_range(const LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e);
+
+}  // namespace tdfs
+
 struct tdfs_graph {
   int device;
   int64_t n;
@@ -123,6 +141,8 @@ struct tdfs_graph {
   int32_t *src;
   int32_t *maxnd;
   uint8_t *label;
+  int32_t *lperm;         // device label index (labeled graphs), see LabelIndex
+  tdfs::LabelIndex *lindex;  // its host copy and group offsets
   tdfs::Workspace *ws;    // launch workspace (pooled; taken at the first launch)
   tdfs::RunCtl *ctl;      // = ws->ctl etc. while a workspace is held
   tdfs::SplitUnit *queue;

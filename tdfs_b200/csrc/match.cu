@@ -740,8 +740,10 @@ struct Engine {
     bool ok = lane < chunk && e < __ldcg(&in.e_end);
     int32_t r = 0, c = 0;
     if (ok) {
-      r = G.src[e];
-      c = G.colidx[e];
+      // labeled plans may walk the label index: positions map to edge ids
+      const int64_t ed = __ldcg(&in.perm) ? (int64_t)G.lperm[e] : e;
+      r = G.src[ed];
+      c = G.colidx[ed];
       if (!LAB && P.orient && !(r < c)) ok = false;
       if (LAB && ok && ((int32_t)G.label[r] != P.label[0] || (int32_t)G.label[c] != P.label[1])) ok = false;
       if (ok && (deg(r) < P.deg[0] || deg(c) < P.deg[1] || G.maxnd[c] < P.deg[2])) ok = false;
@@ -895,10 +897,11 @@ struct Engine {
     const unsigned long long gate = split_gate();
     if (lane < nwarps && lane != me && now - *(volatile const unsigned long long *)&warp_at(lane).t_base >= gate) {
       const WarpSmem &V = warp_at(lane);
+      const int vk = *(volatile const int32_t *)&V.plan.k;
       for (int l = 1; l <= kMaxK - 2; ++l) {
         const unsigned long long w = *(volatile const unsigned long long *)&V.word[l];
         const int rem = (int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu);
-        if (rem >= min_items) {
+        if (rem >= (l >= 2 && l == vk - 2 ? max(min_items, cfg.leaf_min) : min_items)) {
           key = ((unsigned long long)(kMaxK - l) << 40) | ((unsigned long long)rem << 8) | (unsigned)lane;
           break;
         }
@@ -918,7 +921,8 @@ struct Engine {
     w = __shfl_sync(kFull, w, 0);
     __threadfence_block();
     const int it = (int)((uint32_t)(w >> 16) & 0xffffu), n = (int)((uint32_t)w & 0xffffu);
-    if (n - it < min_items) return 0;
+    const int vk = *(volatile const int32_t *)&V.plan.k;
+    if (n - it < (l >= 2 && l == vk - 2 ? max(min_items, cfg.leaf_min) : min_items)) return 0;
     const int vslot = *(volatile int32_t *)&V.slot;
     if (vslot < 0) return 0;
     const int take = (n - it) / 2;
@@ -946,6 +950,9 @@ struct Engine {
       atomicAdd(&tab->hot[vslot].holders, 1);
       won = atomicCAS(&V.word[l], w, (w & ~0xffffull) | (unsigned long long)from) == w;
       if (won) {
+        // the victim's largest grain was just halved: it cools down for a
+        // full gate before it can be split again
+        *(volatile unsigned long long *)&V.t_base = now_ns();
         W.slot = vslot;
       } else {
         release_lane0(vslot);  // nothing to flush: this warp holds no work
@@ -1066,7 +1073,8 @@ struct Engine {
       int l = 1;
       for (; l <= level; ++l) {
         const unsigned long long w = *(volatile unsigned long long *)&W.word[l];
-        if ((int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu) >= 2) break;
+        const int rem = (int)((uint32_t)w & 0xffffu) - (int)((uint32_t)(w >> 16) & 0xffffu);
+        if (rem >= (l >= 2 && l == P.k - 2 ? max(2, cfg.leaf_min) : 2)) break;
       }
       if (l <= level) {
         const long long pos = queue_reserve();
@@ -1225,7 +1233,7 @@ struct Engine {
               }
               count += mode == 2 ? count_free_batch(i, buf(level) + first, b)
                                  : count_fixed_flat(i, buf(level) + first, b);
-              if (cfg.steal) maybe_donate(level);
+              if (cfg.steal && (cfg.budgeted ? (claims & 7u) == 0 : (++claims & 7u) == 0)) maybe_donate(level);
               continue;
             }
           }

@@ -62,6 +62,8 @@ struct KernelCfg {
   int32_t budgeted;     // 1: some slot has a work budget (SlotInfo::budget); warps account their work
   int32_t rush_hungry;  // with at least this many warps idle (0 = never) ...
   int32_t rush_ns;      // ... subtrees may be split after this long instead of split_after_ns
+  int32_t leaf_min;     // the last stored level (its items only count leaves) is split only
+                        // with at least this many items left
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)

@@ -162,15 +162,14 @@ int admit(Server &S, std::vector<Pending> &batch) {
   for (const Pending &q : batch) {
     const int s = S.next_slot++;
     SlotInfo &in = h->info[s];
-    in.e_begin = 0;
-    in.e_end = S.g->nedges;
+    level0_range(S.g, q.plan, 0, S.g->nedges, S.opt.launch.label_index >= 0, &in);
     in.stride = 1;
     in.phase = 0;
-    in.chunk = auto_chunk(S.g->nedges, 1, S.shape.blocks * S.shape.warps_per_block, S.opt.launch.edge_chunk);
-    in.ntickets = (S.g->nedges + in.chunk - 1) / in.chunk;
+    in.chunk = auto_chunk(in.e_end - in.e_begin, 1, S.shape.blocks * S.shape.warps_per_block, S.opt.launch.edge_chunk);
+    in.ntickets = (in.e_end - in.e_begin + in.chunk - 1) / in.chunk;
     in.budget = S.opt.launch.work_budget;
     std::memset(&h->hot[s], 0, sizeof h->hot[s]);
-    h->hot[s].state = kSlotActive;
+    h->hot[s].state = in.ntickets > 0 ? kSlotActive : kSlotDone;  // labels no edge has: done at once
     h->plan[s] = q.plan;
     S.slot_ticket[s] = q.ticket;
     S.slot_bytes[s] = q.bytes;

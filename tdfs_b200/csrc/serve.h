@@ -18,6 +18,10 @@ struct LaunchShape {
 };
 int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options &o, LaunchShape *out);
 
+// The level-0 range of a slot over edge ids [eb, ee), through the graph's
+// label index for labeled plans when use_index is set (capi.cpp).
+void level0_range(const tdfs_graph *g, const DevPlan &p, int64_t eb, int64_t ee, bool use_index, SlotInfo *in);
+
 // The device plan table of a compiled pattern (capi.cpp).
 const DevPlan &plan_device_table(const tdfs_plan *p);
 

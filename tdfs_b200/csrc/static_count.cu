@@ -155,6 +155,7 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   g.src = src;
   g.label = label8;
   g.maxnd = maxnd;
+  g.lperm = nullptr;  // no label index here: labeled slots walk the edge ids
   g.nedges = nedges;
   g.n = (int32_t)n;
   g.max_degree = 0;

@@ -34,6 +34,7 @@ OPTION_SETS = [
     {"lane_list": -1},                     # one warp-wide pass per last-level sibling
     {"split_rush_us": -1, "steal_first": 2},            # no tail rush
     {"split_rush_us": 1, "split_after_us": 400, "fixed_stage": -1},  # long gate, 1 us in the tail
+    {"label_index": -1, "leaf_steal_min": -1},          # labeled level 0 over every edge id; leaves stealable
 ]
 
 
@@ -146,6 +147,26 @@ def test_edge_shards_sum_to_total(er, T, chunk):
     shards = [T.count_batch(er.dev, [P], T.shard_options(r, 4, edge_begin=b, edge_end=e, edge_chunk=chunk))[0][0]
               for r in range(4)]
     assert sum(shards) == part
+
+
+@pytest.mark.parametrize("chunk", [0, 1, 4])
+def test_labeled_ranges_and_shards_through_the_label_index(er, cl, T, chunk):
+    """Labeled level-0 tickets walk the label index; edge ranges and
+    round-robin shards still cover exactly the same edge ids as without it."""
+    rng = random.Random(23)
+    for case in (er, cl):
+        text = random_pattern(5, 0.5, 4, rng)
+        P = T.PatternPreprocessor(text=text, labeled=True)
+        total = T.count(case.dev, P).count
+        assert total == T.count(case.dev, P, T.default_options(label_index=-1)).count
+        E = case.csr.nedges
+        b, e = E // 5, E // 2
+        part = T.count(case.dev, P, T.default_options(edge_begin=b, edge_end=e)).count
+        assert part == T.count(case.dev, P, T.default_options(edge_begin=b, edge_end=e, label_index=-1)).count
+        assert part == case.po.count(case.ora, case.po.Plan(text, True), 0, b, e)
+        shards = [T.count(case.dev, P, T.shard_options(r, 3, edge_begin=b, edge_end=e, edge_chunk=chunk)).count
+                  for r in range(3)]
+        assert sum(shards) == part
 
 
 def test_cli_matches_reference_line_format(T, tmp_path):
