@@ -367,7 +367,8 @@ def run_tdfs(args, rank, world, dist):
     knobs = default
     if not args.no_autotune:
         t0 = time.perf_counter()
-        tuned, sample_ms = T.autotune(G, plans, shard(tune_range, default), sample_stride=4)
+        # whole steps are short here: tune on all of them, else every 4th chunk
+        tuned, sample_ms = T.autotune(G, plans, shard(tune_range, default), sample_stride=1 if slices == 1 else 4)
         tuned.edge_begin, tuned.edge_end = 0, -1
         tune_s = time.perf_counter() - t0
 
@@ -381,8 +382,8 @@ def run_tdfs(args, rank, world, dist):
             return min(ms)
         d_ms, t_ms = trial(default), trial(tuned)
         knobs = tuned if t_ms <= d_ms else default
-        launch = {"autotune": "tdfs_autotune on every 4th level-0 chunk, kept only if faster than the defaults "
-                              "over warm-up steps", "autotune_s": round(tune_s, 2),
+        launch = {"autotune": "tdfs_autotune on a warm-up step (every level-0 chunk of a whole-graph step, every "
+                              "4th of a slice), kept only if faster than the defaults over warm-up steps", "autotune_s": round(tune_s, 2),
                   "tuned": {f: getattr(tuned, f) for f, _ in T.Options._fields_
                             if f not in ("stream", "edge_begin", "edge_end", "edge_stride", "edge_phase")},
                   "warmup_step_ms": {"default": d_ms, "tuned": t_ms}, "chosen": "tuned" if knobs is tuned else "default"}
@@ -434,7 +435,7 @@ def run_tdfs(args, rank, world, dist):
     e2e_knobs = shard((0, -1), knobs)
     e2e_knobs.graph_capture = 0  # a fresh graph every step: nothing to replay
     e2e_s, e2e_m = 0.0, 0
-    for r in timed_r:
+    for s_, r in enumerate([timed_r[0]] + timed_r):  # the first pass is an untimed warm-up step
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         Gh = T.GraphPreprocessor(rowptr=rp.numpy(), colidx=ci.numpy(), labels=None if lb is None else lb.numpy(),
@@ -442,9 +443,11 @@ def run_tdfs(args, rank, world, dist):
         ps = [T.PatternPreprocessor(text=t, labeled=lab) for _, t, lab in pats]
         o = shard(r, e2e_knobs)
         o.graph_capture = 0
-        e2e_m += sum(T.count_batch(Gh, ps, o)[0])
+        m = sum(T.count_batch(Gh, ps, o)[0])
         Gh.close()
-        e2e_s += time.perf_counter() - t0
+        if s_ > 0:
+            e2e_m += m
+            e2e_s += time.perf_counter() - t0
     if dist:
         e2e_s, (e2e_m,) = reduce_over_ranks(dist, e2e_s, [e2e_m])
     modes = len({lab for _, _, lab in pats})

@@ -74,9 +74,9 @@ typedef struct {
                            TDFS_ERR_TIMEOUT; the others complete normally */
   int wait_limit_ms;    /* bound on a warp's idle wait for work before the launch reports
                            TDFS_ERR_TIMEOUT (0 auto = 30000) */
-  int split_rush_us;    /* once a quarter of the grid's warps are idle (the tail of a launch),
+  int split_rush_us;    /* > 0: once a quarter of the grid's warps are idle (the tail of a launch),
                            subtrees may be split after this many microseconds instead of
-                           split_after_us (0 auto = 10, -1 off) */
+                           split_after_us (0 = off) */
   int leaf_steal_min;   /* items of the last stored level (each only counts leaves) are stolen or
                            donated only while at least this many are left (0 auto = 64, -1 = 2) */
   int label_index;      /* labeled plans take level-0 tickets over the graph's label index: only

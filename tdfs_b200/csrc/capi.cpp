@@ -118,12 +118,15 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   const int per_sm = o.blocks_per_sm > 0 ? std::min(o.blocks_per_sm, fit) : fit;
   c.wide_regs = per_sm <= fit_wide ? 1 : 0;
   s.blocks = prop.multiProcessorCount * per_sm;
-  // the tail rush: once a quarter of the grid is idle, split after rush_us
-  if (o.split_rush_us < 0 || c.split_after_ns == 0) {
+  // the tail rush (opt-in): once a quarter of the grid is idle, split after
+  // split_rush_us.  Off by default: on the labeled ER batch (config 3) it
+  // turned 2.4 ms into 3.4 ms -- the extra splits of small subtrees cost more
+  // than the idle time they recover.
+  if (o.split_rush_us <= 0 || c.split_after_ns == 0) {
     c.rush_hungry = 0;
   } else {
     c.rush_hungry = std::max(1, s.blocks * s.warps_per_block / 4);
-    c.rush_ns = (o.split_rush_us > 0 ? o.split_rush_us : 10) * 1000;
+    c.rush_ns = o.split_rush_us * 1000;
     if (c.rush_ns > c.split_after_ns) c.rush_ns = c.split_after_ns;
   }
   *out = s;
@@ -559,7 +562,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::edge_chunk, {1, 4, 8, 32}},
       {&tdfs_options::fixed_stage, {-1, 1}},
       {&tdfs_options::split_after_us, {-1, 5, 50, 150, 500}},
-      {&tdfs_options::split_rush_us, {-1, 2, 10, 40}},
+      {&tdfs_options::split_rush_us, {0, 10, 40}},
       {&tdfs_options::leaf_steal_min, {-1, 16, 64, 256}},
   };
   for (const Knob &k : knobs) {

@@ -32,7 +32,7 @@ OPTION_SETS = [
     {"edge_chunk": 4, "blocks_per_sm": 2, "steal_first": 32},
     {"lane_list": 64, "chunk_cap": 128},   # longer lists in the flattened last-level pass
     {"lane_list": -1},                     # one warp-wide pass per last-level sibling
-    {"split_rush_us": -1, "steal_first": 2},            # no tail rush
+    {"split_rush_us": 10, "steal_first": 2},            # tail rush after 10 us
     {"split_rush_us": 1, "split_after_us": 400, "fixed_stage": -1},  # long gate, 1 us in the tail
     {"label_index": -1, "leaf_steal_min": -1},          # labeled level 0 over every edge id; leaves stealable
 ]
