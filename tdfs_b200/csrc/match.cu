@@ -54,6 +54,7 @@ struct alignas(16) WarpSmem {
   LevelHdr hf;                   // scan of the last vertex's fixed lists
   int32_t fvalid;                // 0: stale, 1: F holds the fixed set, 2: too large
   int32_t fn;                    // |F|
+  int32_t xneq[kMaxK];           // values the last vertex must differ from, between F's anchor and the parent
   unsigned long long t_base;     // globaltimer when the current base work was taken
 };
 
@@ -186,6 +187,7 @@ struct Engine {
   size_t hdr_bytes;     // WarpSmem rounded to 16 bytes
   unsigned long long count = 0;
   unsigned long long work = 0;  // work units since the last flush: one per claim and per 32-wide scan step
+  int hungry_seen = 0;          // lane 0: the idle-warp count as last read (maybe_donate)
   int lane;
 
   __device__ Engine(const DevGraph &g, const KernelCfg &c, RunCtl *ct, SlotTable *tb, SplitUnit *u, QueueHdr *q,
@@ -202,16 +204,34 @@ struct Engine {
 
   // Set up the candidate scan of pattern vertex i from phi(0..i-1).
   __device__ void setup(int i, bool allow_reuse) {
-    if (i == P.k - 2 && lane == 0) W.fvalid = 0;  // the last vertex's fixed lists change with this parent
-    setup_into(W.h[i], i, allow_reuse, -1);
+    // the last vertex's fixed set depends on phi(0..anchor): a new vertex at
+    // the anchor level makes it stale
+    if (lane == 0 && i == fixed_anchor(P.k - 1) + 1) W.fvalid = 0;
+    setup_into(W.h[i], i, allow_reuse, i - 1);
   }
 
-  // Set up a scan for vertex i into header H; `excl` >= 0 leaves that earlier
-  // vertex out of the backward neighbours and the conditions (the fixed part
-  // of the last vertex's candidate set, see count_fixed).
-  __device__ void setup_into(LevelHdr &H, int i, bool allow_reuse, int excl) {
+  // The level the last vertex i's fixed set F hangs on: its deepest backward
+  // neighbour other than the parent (vertex i-1), at least 1 (level-1 items
+  // change phi(0) and phi(1) together).  F is built with the backward
+  // neighbours and conditions of vertices up to the anchor only, so it stays
+  // valid for every node below the anchor; the conditions on the vertices
+  // between the anchor and the parent are applied per count (extra_conds).
+  __device__ int fixed_anchor(int i) const {
+    int a = 1;
+    for (int t = 0; t < P.nbn[i]; ++t) {
+      const int b = P.bn[i][t];
+      if (b != i - 1 && b > a) a = b;
+    }
+    return a;
+  }
+
+  // Set up a scan for vertex i into header H over the backward neighbours and
+  // conditions of the vertices up to `limit` (i - 1: all of them; smaller:
+  // the fixed part of the last vertex's candidate set, see build_fixed).
+  __device__ void setup_into(LevelHdr &H, int i, bool allow_reuse, int limit) {
     const int dep = P.dep[i];
-    const bool reuse = excl < 0 && allow_reuse && dep >= 2 && W.h[dep].complete;
+    const bool full = limit >= i - 1;
+    const bool reuse = full && allow_reuse && dep >= 2 && W.h[dep].complete;
     const int32_t *src;
     int32_t slen;
     int nm = 0;
@@ -233,7 +253,7 @@ struct Engine {
       // scan the smallest backward-neighbour list (first on ties, as
       // src/gpu_match.cu:646-663)
       const int nbn = P.nbn[i];
-      const bool part = lane < nbn && P.bn[i][lane] != excl;
+      const bool part = lane < nbn && P.bn[i][lane] <= limit;
       const unsigned pmask = __ballot_sync(kFull, part);
       unsigned long long key = ~0ull;
       int64_t b = 0, e = 0;
@@ -269,7 +289,7 @@ struct Engine {
     int32_t lo = -1, hi = INT_MAX;
     bool isneq = false;
     int32_t myphi = 0;
-    if (lane < i && lane != excl) {
+    if (lane < i && lane <= limit) {
       myphi = W.phi[lane];
       if (LAB) {
         isneq = true;
@@ -289,7 +309,7 @@ struct Engine {
     // skip the prefix <= lo by a 32-ary search; a short source is cheaper to
     // filter in the scan, except when the closed-form count needs the bound
     int32_t spos = 0;
-    const bool closed = !LAB && nm == 0 && hi == INT_MAX && i == P.k - 1 && excl < 0;
+    const bool closed = !LAB && nm == 0 && hi == INT_MAX && i == P.k - 1 && full;
     if (!LAB && lo >= 0 && slen > 0 && (slen > 64 || closed)) spos = warp_upper_bound(src, 0, slen, lo);
     // merge (staged window) or per-lane search, per list, by degree ratio
     uint32_t mm = 0;
@@ -373,7 +393,7 @@ struct Engine {
 
   __device__ void build_fixed(int i) {
     LevelHdr &H = W.hf;
-    setup_into(H, i, false, i - 1);
+    setup_into(H, i, false, fixed_anchor(i));
     int32_t *out = fbuf();
     const int32_t *src = H.src;
     const int32_t send = H.send;
@@ -405,9 +425,58 @@ struct Engine {
     __syncwarp();
   }
 
+  // Conditions of the last vertex i on the vertices between F's anchor and
+  // its parent, (anchor, i-2], for the current prefix: a lower and an upper
+  // bound (unlabeled symmetry conditions) and the values it must differ from
+  // (W.xneq[0..n)).  F was built without them; they are applied per count.
+  struct Extra {
+    int32_t lo, hi;
+    int n;
+  };
+
+  __device__ Extra extra_conds(int i) {
+    const int a = fixed_anchor(i);
+    int32_t lo = -1, hi = INT_MAX, v = 0;
+    bool isneq = false;
+    if (lane > a && lane <= i - 2) {
+      v = W.phi[lane];
+      if (LAB) {
+        isneq = true;
+      } else if (P.larger[i] >> lane & 1) {
+        lo = v;
+      } else if (P.less[i] >> lane & 1) {
+        hi = v;
+      } else {
+        isneq = true;
+      }
+    }
+    Extra X;
+    X.lo = (int32_t)__reduce_max_sync(kFull, (unsigned)(lo + 1)) - 1;
+    X.hi = (int32_t)__reduce_min_sync(kFull, (unsigned)hi);
+    const unsigned m = __ballot_sync(kFull, isneq);
+    if (isneq) W.xneq[__popc(m & lanemask_lt())] = v;
+    X.n = __popc(m);
+    __syncwarp();
+    return X;
+  }
+
+  __device__ __forceinline__ bool extra_ok(const Extra &X, int32_t y) const {
+    if (y <= X.lo || y >= X.hi) return false;
+    for (int t = 0; t < X.n; ++t)
+      if (W.xneq[t] == y) return false;
+    return true;
+  }
+
+  __device__ __forceinline__ bool in_fixed(int32_t y) {
+    const int32_t *F = fbuf();
+    const int32_t q = lower_bound(F, 0, W.fn, y);
+    return q < W.fn && F[q] == y;
+  }
+
   __device__ unsigned long long count_fixed(int i) {
     const int32_t x = W.phi[i - 1];
     if (W.fn == 0) return 0;
+    const Extra X = extra_conds(i);
     int64_t b = 0, e = 0;
     if (lane == 0) {
       b = G.rowptr[x];
@@ -415,7 +484,7 @@ struct Engine {
     }
     b = __shfl_sync(kFull, b, 0);
     e = __shfl_sync(kFull, e, 0);
-    return count_fixed_list(i, x, b, e);
+    return count_fixed_list(i, x, b, e, X);
   }
 
   // The condition between the last vertex i and its parent: 1 = y > x,
@@ -438,6 +507,7 @@ struct Engine {
     const int32_t nF = W.fn;
     if (nF == 0) return 0;
     const int rel = parent_rel(i);
+    const Extra X = extra_conds(i);
     const bool mine = lane < b;
     const int32_t x = mine ? items[lane] : 0;
     int64_t rb = 0, re = 0;
@@ -480,7 +550,7 @@ struct Engine {
 #pragma unroll
       for (int u = 0; u < kFlatUnroll; ++u) {
         const int32_t yy = y[u], xx = xo[u];
-        if (v[u] && (rel == 1 ? yy > xx : rel == 2 ? yy < xx : yy != xx)) {
+        if (v[u] && (rel == 1 ? yy > xx : rel == 2 ? yy < xx : yy != xx) && extra_ok(X, yy)) {
           const int32_t q = lower_bound(F, 0, nF, yy);
           c += q < nF && F[q] == yy;
         }
@@ -491,18 +561,19 @@ struct Engine {
     while (rest) {
       const int j = __ffs(rest) - 1;
       rest &= rest - 1;
-      sum += count_fixed_list(i, __shfl_sync(kFull, x, j), __shfl_sync(kFull, rb, j), __shfl_sync(kFull, re, j));
+      sum += count_fixed_list(i, __shfl_sync(kFull, x, j), __shfl_sync(kFull, rb, j), __shfl_sync(kFull, re, j), X);
     }
     return sum;
   }
 
   // The last vertex i when its parent (vertex i-1) is not one of its backward
-  // neighbours: its whole candidate set C (F, built once per grandparent by
-  // build_fixed with every condition except the one on the parent) is the
-  // same for all siblings at level i-1, and sibling x counts the elements of
-  // C that satisfy that one condition: y > x, y < x, or y != x (unlabeled
-  // symmetry conditions, or injectivity when labeled).  C is sorted, so each
-  // sibling is one binary search in shared memory; lane j takes sibling j.
+  // neighbours: its candidate set is F (built once per anchor-level node by
+  // build_fixed) cut by the conditions on the vertices after the anchor --
+  // the fixed ones between the anchor and the parent (extra_conds) and the
+  // parent's own (y > x, y < x, or y != x: unlabeled symmetry conditions, or
+  // injectivity when labeled).  F is sorted, so sibling x counts a range of
+  // F by two binary searches in shared memory, less the excluded values that
+  // fall in it; lane j takes sibling j.
   __device__ bool free_applies(int i) {
     if (!cfg.fixed || i < 3) return false;
     for (int t = 0; t < P.nbn[i]; ++t)
@@ -515,24 +586,30 @@ struct Engine {
     const int32_t nF = W.fn;
     if (nF == 0) return 0;
     const int rel = parent_rel(i);
+    const Extra X = extra_conds(i);
     unsigned c = 0;
     if (lane < b) {
       const int32_t x = items[lane];
-      if (rel == 1) {
-        c = (unsigned)(nF - upper_bound_smem(F, nF, x));
-      } else if (rel == 2) {
-        c = (unsigned)lower_bound(F, 0, nF, x);
-      } else {
-        const int32_t q = lower_bound(F, 0, nF, x);
-        c = (unsigned)(nF - (q < nF && F[q] == x ? 1 : 0));
+      int32_t lo = X.lo, hi = X.hi;  // candidates lie strictly between
+      if (rel == 1) lo = max(lo, x);
+      else if (rel == 2) hi = min(hi, x);
+      int32_t cnt = 0;
+      if (lo < hi) {
+        cnt = max(0, lower_bound(F, 0, nF, hi) - upper_bound_smem(F, nF, lo));
+        for (int t = 0; t < X.n; ++t) {
+          const int32_t e = W.xneq[t];
+          if (e > lo && e < hi && in_fixed(e)) --cnt;
+        }
+        if (rel == 0 && x > lo && x < hi && in_fixed(x)) --cnt;
       }
+      c = (unsigned)cnt;
     }
     return __reduce_add_sync(kFull, c);
   }
 
   // |F ∩ N(x)| under the parent condition, the warp together; N(x) is
   // colidx[b, e).
-  __device__ unsigned long long count_fixed_list(int i, int32_t x, int64_t b, int64_t e) {
+  __device__ unsigned long long count_fixed_list(int i, int32_t x, int64_t b, int64_t e, const Extra &X) {
     const int32_t *F = fbuf();
     const int32_t nF = W.fn;
     const int32_t *L = G.colidx + b;
@@ -548,7 +625,7 @@ struct Engine {
         const int32_t idx = pos + lane;
         const bool valid = idx < len;
         const int32_t y = valid ? L[idx] : 0;
-        bool ok = valid && (rel == 1 ? y > x : rel == 2 ? y < x : y != x);
+        bool ok = valid && (rel == 1 ? y > x : rel == 2 ? y < x : y != x) && extra_ok(X, y);
         if (ok) {
           const int32_t q = lower_bound(F, 0, nF, y);
           ok = q < nF && F[q] == y;
@@ -564,7 +641,7 @@ struct Engine {
         const int32_t idx = pos + lane;
         const bool valid = idx < nF;
         const int32_t y = valid ? F[idx] : 0;
-        bool ok = valid && (rel == 1 ? y > x : rel == 2 ? y < x : y != x);
+        bool ok = valid && (rel == 1 ? y > x : rel == 2 ? y < x : y != x) && extra_ok(X, y);
         const bool searched = ok;
         int32_t p = 0;
         if (ok) {
@@ -638,7 +715,7 @@ struct Engine {
   __device__ int32_t claim_batch(int l, int *b) {
     int32_t r = -1, got = 0;
     if (lane == 0) {
-      const bool share = cfg.steal && *(volatile int32_t *)&ctl->hungry > 0;
+      const bool share = cfg.steal && hungry_seen > 0;
       unsigned long long w = *(volatile unsigned long long *)&W.word[l];
       for (int tries = 0;; ++tries) {
         const uint32_t it = (uint32_t)(w >> 16) & 0xffffu, n = (uint32_t)w & 0xffffu;
@@ -647,7 +724,9 @@ struct Engine {
           raise_error(ctl, TDFS_ERR_TIMEOUT);
           break;
         }
-        const uint32_t take = min(32u, share ? max(1u, (n - it) / 2) : n - it);
+        // leaving half only helps while what is left can still be stolen
+        const bool half = share && n - it >= 2u * (uint32_t)cfg.leaf_min;
+        const uint32_t take = min(32u, half ? max(1u, (n - it) / 2) : n - it);
         const unsigned long long old = atomicCAS(&W.word[l], w, w + ((unsigned long long)take << 16));
         if (old == w) {
           r = (int32_t)it;
@@ -1066,7 +1145,12 @@ struct Engine {
   // shallowest remaining items into the global ring.
   __device__ void maybe_donate(int level) {
     int hungry = 0;
-    if (lane == 0 && now_ns() - W.t_base >= 4ull * split_gate()) hungry = *(volatile int32_t *)&ctl->hungry;
+    if (lane == 0) {
+      // the one read of the grid-wide idle count on the busy path, every few
+      // claims; claim_batch works from this copy
+      hungry_seen = *(volatile int32_t *)&ctl->hungry;
+      if (now_ns() - W.t_base >= 4ull * split_gate()) hungry = hungry_seen;
+    }
     hungry = __shfl_sync(kFull, hungry, 0);
     if (hungry <= 0) return;
     if (lane == 0) {
