@@ -82,6 +82,10 @@ typedef struct {
   int label_index;      /* labeled plans take level-0 tickets over the graph's label index: only
                            the edges whose end labels match the plan's first two vertices
                            (0 auto = on, -1 off: every edge id, filtered) */
+  int level_hoist;      /* a stored level whose backward neighbours all lie above its parent keeps
+                           its candidate set (as of its deepest backward neighbour) and reuses it
+                           for every node below, cut by the conditions in between
+                           (0 auto = on, -1 off) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

@@ -76,6 +76,7 @@ class Options(C.Structure):
         ("split_rush_us", C.c_int),
         ("leaf_steal_min", C.c_int),
         ("label_index", C.c_int),
+        ("level_hoist", C.c_int),
     ]
 
 

@@ -80,6 +80,7 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.steal_min = o.steal_min > 0 ? o.steal_min : 2;
   c.steal_first = o.steal_first > 0 ? o.steal_first : 8;
   c.leaf_min = o.leaf_steal_min > 0 ? o.leaf_steal_min : (o.leaf_steal_min < 0 ? 2 : 64);
+  c.hoist = o.level_hoist < 0 ? 0 : 1;
   c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 32);
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
@@ -564,6 +565,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::split_after_us, {-1, 5, 50, 150, 500}},
       {&tdfs_options::split_rush_us, {0, 10, 40}},
       {&tdfs_options::leaf_steal_min, {-1, 16, 64, 256}},
+      {&tdfs_options::level_hoist, {-1, 1}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {

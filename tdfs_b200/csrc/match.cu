@@ -39,7 +39,7 @@ struct LevelHdr {
   int32_t nprod;                 // candidates produced into the buffer (first fill)
   int32_t complete;              // buffer holds the whole candidate set
   uint32_t merge_mask;           // bit m: list m uses the staged-window merge
-  int32_t pad_;
+  int32_t core;                  // hoisted level: the buffer holds the level's core set (see hoist_anchor)
 };
 
 struct alignas(16) WarpSmem {
@@ -204,10 +204,88 @@ struct Engine {
 
   // Set up the candidate scan of pattern vertex i from phi(0..i-1).
   __device__ void setup(int i, bool allow_reuse) {
-    // the last vertex's fixed set depends on phi(0..anchor): a new vertex at
-    // the anchor level makes it stale
-    if (lane == 0 && i == fixed_anchor(P.k - 1) + 1) W.fvalid = 0;
+    stale_from(i - 1);
     setup_into(W.h[i], i, allow_reuse, i - 1);
+  }
+
+  // phi(j) just changed: the sets built on phi(0..j) -- the last vertex's
+  // fixed set and the core sets of hoisted levels anchored at j or deeper --
+  // are stale.
+  __device__ void stale_from(int j) {
+    if (lane == 0) {
+      if (fixed_anchor(P.k - 1) >= j) W.fvalid = 0;
+      for (int t = j + 1; t <= P.k - 2; ++t)
+        if (hoist_anchor(t) >= j) W.h[t].core = 0;
+    }
+  }
+
+  // ---- hoisted levels --------------------------------------------------------
+  // A stored level i whose backward neighbours all lie at or above level a <
+  // i - 1 (a = its deepest one, at least 1) has a candidate set that depends
+  // on phi(0..a) only, except for the conditions on the vertices between a
+  // and i: the "core" set -- the backward neighbours' lists intersected and
+  // filtered by the conditions on phi(0..a) -- is produced once per node at
+  // level a into the level's buffer and reused for every node below it.  Each
+  // reuse publishes the sub-range of the sorted core set inside the bounds of
+  // the conditions between a and i (two searches in shared memory); values
+  // that must differ from one of those vertices are skipped when claimed
+  // (item_ok).  Returns a, or -1 when level i is not hoisted.
+  __device__ int hoist_anchor(int i) const {
+    if (!cfg.hoist || i < 2 || i > P.k - 2 || P.dep[i] >= 0) return -1;
+    int a = 1;
+    for (int t = 0; t < P.nbn[i]; ++t) a = max(a, (int)P.bn[i][t]);
+    return a < i - 1 ? a : -1;
+  }
+
+  // Lane-wise: may candidate x of level l be claimed under the current
+  // prefix?  Only a hoisted level has candidates that can fail: those equal
+  // to a vertex between the anchor and l that l must differ from.
+  __device__ __forceinline__ bool item_ok(int l, int32_t x) const {
+    const int a = hoist_anchor(l);
+    if (a < 0) return true;
+    for (int j = a + 1; j < l; ++j) {
+      const bool neq = LAB || !((P.larger[l] | P.less[l]) >> j & 1);
+      if (neq && W.phi[j] == x) return false;
+    }
+    return true;
+  }
+
+  // Produce level i's core set into its buffer when the smallest source list
+  // fits (the whole set then lands in one chunk); false otherwise, and the
+  // caller produces the level the ordinary way.
+  __device__ bool build_core(int i, int a) {
+    LevelHdr &H = W.h[i];
+    setup_into(H, i, false, a);
+    if (H.send - H.spos > cfg.cap - 32) return false;
+    produce(i);
+    if (lane == 0) {
+      H.core = 1;
+      H.complete = 0;  // not the candidate set of the current prefix: no reuse from it
+    }
+    __syncwarp();
+    return true;
+  }
+
+  // Publish the part of level i's core set inside the bounds of the
+  // conditions on the vertices between the anchor a and i.
+  __device__ void publish_core(int i, int a) {
+    int32_t lo = -1, hi = INT_MAX;
+    if (!LAB && lane > a && lane < i) {
+      if (P.larger[i] >> lane & 1) lo = W.phi[lane];
+      else if (P.less[i] >> lane & 1) hi = W.phi[lane];
+    }
+    lo = (int32_t)__reduce_max_sync(kFull, (unsigned)(lo + 1)) - 1;
+    hi = (int32_t)__reduce_min_sync(kFull, (unsigned)hi);
+    if (lane == 0) {
+      const int32_t *c = buf(i);
+      const int32_t n = W.h[i].nprod;
+      const int32_t b = lo >= 0 ? upper_bound_smem(c, n, lo) : 0;
+      const int32_t e = hi < INT_MAX ? lower_bound(c, 0, n, hi) : n;
+      const unsigned long long gen = (W.word[i] >> 32) + 1;
+      __threadfence_block();
+      atomicExch(&W.word[i], (gen << 32) | ((unsigned long long)b << 16) | (unsigned long long)max(b, e));
+    }
+    __syncwarp();
   }
 
   // The level the last vertex i's fixed set F hangs on: its deepest backward
@@ -508,7 +586,7 @@ struct Engine {
     if (nF == 0) return 0;
     const int rel = parent_rel(i);
     const Extra X = extra_conds(i);
-    const bool mine = lane < b;
+    const bool mine = lane < b && item_ok(i - 1, items[lane]);
     const int32_t x = mine ? items[lane] : 0;
     int64_t rb = 0, re = 0;
     if (mine) {
@@ -588,7 +666,7 @@ struct Engine {
     const int rel = parent_rel(i);
     const Extra X = extra_conds(i);
     unsigned c = 0;
-    if (lane < b) {
+    if (lane < b && item_ok(i - 1, items[lane])) {
       const int32_t x = items[lane];
       int32_t lo = X.lo, hi = X.hi;  // candidates lie strictly between
       if (rel == 1) lo = max(lo, x);
@@ -838,7 +916,7 @@ struct Engine {
     if (lane == 0) {
       W.fvalid = 0;
       W.t_base = now_ns();
-      for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
+      for (int j = 2; j < kMaxK; ++j) W.h[j].complete = W.h[j].core = 0;
       publish(1, __popc(mask));
     }
     __syncwarp();
@@ -940,7 +1018,7 @@ struct Engine {
     if (lane == 0) {
       W.fvalid = 0;
       W.t_base = now_ns();
-      for (int j = 2; j < kMaxK; ++j) W.h[j].complete = 0;
+      for (int j = 2; j < kMaxK; ++j) W.h[j].complete = W.h[j].core = 0;
       if (l >= 2) {
         W.h[l].spos = W.h[l].send = 0;  // no source left: only the given candidates
         W.h[l].nprod = cnt;
@@ -1234,7 +1312,7 @@ struct Engine {
     unsigned claims = 0;
     if (lane == 0) {
       for (int l = 0; l < kStoredMax; ++l) W.word[l] = 0;
-      for (int l = 0; l < kMaxK; ++l) W.h[l].complete = 0;
+      for (int l = 0; l < kMaxK; ++l) W.h[l].complete = W.h[l].core = 0;
       W.slot = -1;
       W.fvalid = 0;
       W.t_base = 0;
@@ -1335,6 +1413,7 @@ struct Engine {
         } else {
           const int32_t x = buf(level)[idx];
           __syncwarp();
+          if (!item_ok(level, x)) continue;  // a hoisted core value this prefix excludes
           if (lane == 0) W.phi[level] = x;
         }
         __syncwarp();
@@ -1350,8 +1429,15 @@ struct Engine {
         if (level + 1 == P.k - 1) {
           count += count_last(P.k - 1);
         } else {
-          setup(level + 1, true);
-          produce(level + 1);
+          const int i = level + 1;
+          const int a = hoist_anchor(i);
+          stale_from(level);
+          if (a >= 0 && (W.h[i].core || build_core(i, a))) {
+            publish_core(i, a);
+          } else {
+            setup(i, true);
+            produce(i);
+          }
           ++level;
         }
         continue;

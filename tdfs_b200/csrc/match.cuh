@@ -64,6 +64,7 @@ struct KernelCfg {
   int32_t rush_ns;      // ... subtrees may be split after this long instead of split_after_ns
   int32_t leaf_min;     // the last stored level (its items only count leaves) is split only
                         // with at least this many items left
+  int32_t hoist;        // 1: levels whose candidates hang on an ancestor reuse a core set
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)
