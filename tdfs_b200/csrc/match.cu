@@ -217,6 +217,7 @@ struct Engine {
       for (int t = j + 1; t <= P.k - 2; ++t)
         if (hoist_anchor(t) >= j) W.h[t].core = 0;
     }
+    __syncwarp();  // every lane reads the flags next, to take the same path
   }
 
   // ---- hoisted levels --------------------------------------------------------
