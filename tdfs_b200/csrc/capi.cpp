@@ -531,11 +531,13 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
   cur.edge_stride = sample_stride;
   cur.edge_phase = 0;
   std::vector<uint64_t> counts(nplans);
+  std::vector<int> status(nplans);
   auto measure = [&](const tdfs_options &o, float *out) -> int {
     float bestt = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {
       float ms = 0.f;
-      int rc = tdfs_count_batch(g, plans, nplans, &o, counts.data(), &ms);
+      // a plan that runs out of a work budget is timed like the others
+      int rc = tdfs_count_batch_status(g, plans, nplans, &o, counts.data(), status.data(), &ms);
       if (rc) return rc;
       bestt = std::min(bestt, ms);
     }

@@ -55,7 +55,21 @@ struct alignas(16) WarpSmem {
   int32_t fvalid;                // 0: stale, 1: F holds the fixed set, 2: too large
   int32_t fn;                    // |F|
   int32_t xneq[kMaxK];           // values the last vertex must differ from, between F's anchor and the parent
+  // derived from the plan once per plan switch (derive_plan)
+  int8_t hanchor[kMaxK];         // per level: anchor of a hoisted level, -1 when not hoisted
+  uint8_t hneq[kMaxK];           // per hoisted level: bit j = candidates must differ from phi(j)
+  int8_t fanchor;                // anchor of the last vertex's fixed set
+  int8_t lastmode;               // last vertex: 2 parent-free fixed set, 1 fixed set with the parent, 0 neither
+  uint8_t hoistmask;             // bit i: level i is hoisted
+  int8_t pad_d_;
   unsigned long long t_base;     // globaltimer when the current base work was taken
+  // lane 0's bookkeeping, kept here rather than in registers every lane holds
+  unsigned long long idle_since; // bounded idle wait: start of the current wait
+  unsigned long long idle_start; // diagnostics: start of the current idle span
+  unsigned long long idle_total; // diagnostics: idle time so far
+  unsigned long long t_start;    // diagnostics: when this warp started
+  int32_t hungry_seen;           // the grid's idle-warp count as last read (maybe_donate)
+  int32_t pad_h_;
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
@@ -186,8 +200,7 @@ struct Engine {
   unsigned char *cta;   // this CTA's shared memory (warp regions cfg.warp_bytes apart)
   size_t hdr_bytes;     // WarpSmem rounded to 16 bytes
   unsigned long long count = 0;
-  unsigned long long work = 0;  // work units since the last flush: one per claim and per 32-wide scan step
-  int hungry_seen = 0;          // lane 0: the idle-warp count as last read (maybe_donate)
+  unsigned work = 0;  // work units since the last flush: one per claim and per 32-wide scan step
   int lane;
 
   __device__ Engine(const DevGraph &g, const KernelCfg &c, RunCtl *ct, SlotTable *tb, SplitUnit *u, QueueHdr *q,
@@ -213,9 +226,13 @@ struct Engine {
   // are stale.
   __device__ void stale_from(int j) {
     if (lane == 0) {
-      if (fixed_anchor(P.k - 1) >= j) W.fvalid = 0;
-      for (int t = j + 1; t <= P.k - 2; ++t)
-        if (hoist_anchor(t) >= j) W.h[t].core = 0;
+      if (W.fanchor >= j) W.fvalid = 0;
+      unsigned m = (unsigned)W.hoistmask >> (j + 1) << (j + 1);
+      while (m) {
+        const int t = __ffs(m) - 1;
+        m &= m - 1;
+        if (W.hanchor[t] >= j) W.h[t].core = 0;
+      }
     }
     __syncwarp();  // every lane reads the flags next, to take the same path
   }
@@ -231,22 +248,48 @@ struct Engine {
   // the conditions between a and i (two searches in shared memory); values
   // that must differ from one of those vertices are skipped when claimed
   // (item_ok).  Returns a, or -1 when level i is not hoisted.
-  __device__ int hoist_anchor(int i) const {
+  __device__ int hoist_anchor_of(int i) const {
     if (!cfg.hoist || i < 2 || i > P.k - 2 || P.dep[i] >= 0) return -1;
     int a = 1;
     for (int t = 0; t < P.nbn[i]; ++t) a = max(a, (int)P.bn[i][t]);
     return a < i - 1 ? a : -1;
+  }
+  __device__ __forceinline__ int hoist_anchor(int i) const { return W.hanchor[i]; }
+
+  // The plan's derived tables (anchors, masks, last-level mode), written by
+  // lane 0 whenever W.plan changes, so the DFS loop reads them instead of
+  // recomputing them from the plan at every node.
+  __device__ void derive_plan() {
+    if (lane == 0) {
+      unsigned hm = 0;
+      for (int i = 0; i < kMaxK; ++i) {
+        const int a = hoist_anchor_of(i);
+        W.hanchor[i] = (int8_t)a;
+        unsigned m = 0;
+        if (a >= 0) {
+          hm |= 1u << i;
+          for (int j = a + 1; j < i; ++j)
+            if (LAB || !((P.larger[i] | P.less[i]) >> j & 1)) m |= 1u << j;
+        }
+        W.hneq[i] = (uint8_t)m;
+      }
+      W.hoistmask = (uint8_t)hm;
+      const int last = P.k - 1;
+      W.fanchor = (int8_t)fixed_anchor(last);
+      W.lastmode = (int8_t)(free_applies(last) ? 2 : fixed_applies(last) ? 1 : 0);
+    }
+    __syncwarp();
   }
 
   // Lane-wise: may candidate x of level l be claimed under the current
   // prefix?  Only a hoisted level has candidates that can fail: those equal
   // to a vertex between the anchor and l that l must differ from.
   __device__ __forceinline__ bool item_ok(int l, int32_t x) const {
-    const int a = hoist_anchor(l);
-    if (a < 0) return true;
-    for (int j = a + 1; j < l; ++j) {
-      const bool neq = LAB || !((P.larger[l] | P.less[l]) >> j & 1);
-      if (neq && W.phi[j] == x) return false;
+    unsigned m = W.hneq[l];
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      if (W.phi[j] == x) return false;
     }
     return true;
   }
@@ -472,7 +515,7 @@ struct Engine {
 
   __device__ void build_fixed(int i) {
     LevelHdr &H = W.hf;
-    setup_into(H, i, false, fixed_anchor(i));
+    setup_into(H, i, false, W.fanchor);
     int32_t *out = fbuf();
     const int32_t *src = H.src;
     const int32_t send = H.send;
@@ -514,7 +557,7 @@ struct Engine {
   };
 
   __device__ Extra extra_conds(int i) {
-    const int a = fixed_anchor(i);
+    const int a = W.fanchor;
     int32_t lo = -1, hi = INT_MAX, v = 0;
     bool isneq = false;
     if (lane > a && lane <= i - 2) {
@@ -744,7 +787,7 @@ struct Engine {
   }
 
   __device__ unsigned long long count_last(int i) {
-    if (fixed_applies(i)) {
+    if (W.lastmode == 1) {
       if (W.fvalid == 0) build_fixed(i);
       if (W.fvalid == 1) return count_fixed(i);
     }
@@ -794,7 +837,7 @@ struct Engine {
   __device__ int32_t claim_batch(int l, int *b) {
     int32_t r = -1, got = 0;
     if (lane == 0) {
-      const bool share = cfg.steal && hungry_seen > 0;
+      const bool share = cfg.steal && W.hungry_seen > 0;
       unsigned long long w = *(volatile unsigned long long *)&W.word[l];
       for (int tries = 0;; ++tries) {
         const uint32_t it = (uint32_t)(w >> 16) & 0xffffu, n = (uint32_t)w & 0xffffu;
@@ -862,6 +905,7 @@ struct Engine {
     for (int t = lane; t < (int)(sizeof(DevPlan) / 4); t += 32) dstw[t] = __ldcg(srcw + t);
     if (lane == 0) W.slot = s;
     __syncwarp();
+    derive_plan();
   }
 
   // Give up this warp's hold on slot s (lane 0).  Its count is added first;
@@ -1120,6 +1164,7 @@ struct Engine {
     won = __shfl_sync(kFull, won, 0);
     __syncwarp();
     if (!won) return 0;
+    derive_plan();  // the plan came from the victim
     install(l, take);
     if (lane == 0) atomicAdd(&ctl->steals, 1ull);
     return l;
@@ -1227,8 +1272,8 @@ struct Engine {
     if (lane == 0) {
       // the one read of the grid-wide idle count on the busy path, every few
       // claims; claim_batch works from this copy
-      hungry_seen = *(volatile int32_t *)&ctl->hungry;
-      if (now_ns() - W.t_base >= 4ull * split_gate()) hungry = hungry_seen;
+      W.hungry_seen = *(volatile int32_t *)&ctl->hungry;
+      if (now_ns() - W.t_base >= 4ull * split_gate()) hungry = W.hungry_seen;
     }
     hungry = __shfl_sync(kFull, hungry, 0);
     if (hungry <= 0) return;
@@ -1282,7 +1327,7 @@ struct Engine {
       SlotHot &h = tab->hot[s];
       const long long budget = __ldcg(&tab->info[s].budget);
       if (budget > 0) {
-        const unsigned long long tot = atomicAdd(&h.work, work) + work;
+        const unsigned long long tot = atomicAdd(&h.work, (unsigned long long)work) + work;
         if ((long long)tot > budget && atomicCAS(&h.aborted, 0, 1) == 0)
           atomicMax(&h.ticket, (unsigned long long)__ldcg(&tab->info[s].ntickets));
         ab = *(volatile int32_t *)&h.aborted;
@@ -1307,7 +1352,7 @@ struct Engine {
   // tickets of an open slot, a steal from its CTA, or a unit from the ring).
   __device__ void run(int nwarps, int me) {
     int level = 0, base = 1;
-    if (lane == 0) t_start = now_ns();
+    if (lane == 0) W.t_start = now_ns();
     bool hungry = false;  // counted in ctl->hungry (warps polling for work)
     bool holding = false;
     unsigned claims = 0;
@@ -1317,6 +1362,8 @@ struct Engine {
       W.slot = -1;
       W.fvalid = 0;
       W.t_base = 0;
+      W.idle_since = W.idle_start = W.idle_total = 0;
+      W.hungry_seen = 0;
     }
     __syncwarp();
     for (;;) {
@@ -1350,10 +1397,12 @@ struct Engine {
           holding = true;
           if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
           hungry = false;
-          idle_since = 0;
-          if (lane == 0 && idle_start) {
-            idle_total += now_ns() - idle_start;
-            idle_start = 0;
+          if (lane == 0) {
+            W.idle_since = 0;
+            if (W.idle_start) {
+              W.idle_total += now_ns() - W.idle_start;
+              W.idle_start = 0;
+            }
           }
           nap = 256;
           continue;
@@ -1381,7 +1430,7 @@ struct Engine {
         // last stored level: batches of up to 32 siblings against the fixed
         // part of the last vertex's candidates (built once per grandparent)
         const int i = level + 1;
-        const int mode = free_applies(i) ? 2 : (cfg.lane_list > 0 && fixed_applies(i)) ? 1 : 0;
+        const int mode = W.lastmode == 2 ? 2 : (cfg.lane_list > 0 && W.lastmode == 1) ? 1 : 0;
         if (mode) {
           if (W.fvalid == 0) build_fixed(i);
           if (W.fvalid == 1) {
@@ -1452,9 +1501,9 @@ struct Engine {
     if (hungry && lane == 0) atomicSub(&ctl->hungry, 1);
     if (lane == 0) {
       const unsigned long long t = now_ns();
-      if (idle_start) idle_total += t - idle_start;
-      atomicAdd(&ctl->idle_ns, idle_total);
-      atomicAdd(&ctl->warp_ns, t - t_start);
+      if (W.idle_start) W.idle_total += t - W.idle_start;
+      atomicAdd(&ctl->idle_ns, W.idle_total);
+      atomicAdd(&ctl->warp_ns, t - W.t_start);
     }
     __syncwarp();
   }
@@ -1464,23 +1513,21 @@ struct Engine {
   // admissions are closed that means a busy warp stalled and is reported as
   // a timeout; a serving launch simply retires and the host relaunches it.
   unsigned nap = 256;
-  unsigned long long idle_since = 0;
-  unsigned long long idle_start = 0, idle_total = 0, t_start = 0;  // diagnostics (lane 0)
   __device__ bool wait_for_work() {
     int ok = 1;
     if (lane == 0) {
       const unsigned long long t = now_ns();
-      if (!idle_since) idle_since = t;
-      if (!idle_start) idle_start = t;
+      if (!W.idle_since) W.idle_since = t;
+      if (!W.idle_start) W.idle_start = t;
       const SlotCtl &C = tab->ctl;
       const int shut = *(volatile int32_t *)&C.shutdown;
       // serving: the idle clock runs only while every admitted query is
       // complete -- a warp that retired while one query was still running
       // would leave the grid short for the queries admitted after it
       if (!shut && *(volatile unsigned long long *)&C.completed < *(volatile unsigned long long *)&C.admitted)
-        idle_since = t;
+        W.idle_since = t;
       const unsigned long long limit_ms = shut ? (unsigned long long)cfg.idle_ms : (unsigned long long)C.idle_exit_ms;
-      if (t - idle_since > limit_ms * 1000000ull) {
+      if (t - W.idle_since > limit_ms * 1000000ull) {
         if (shut) raise_error(ctl, TDFS_ERR_TIMEOUT);
         ok = 0;
       }
