@@ -11,6 +11,7 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <functional>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -82,6 +83,31 @@ bool is_automorphism(const HostPlan &p, const Perm &pp) {
   return true;
 }
 
+// Every permutation pp of 0..k-1 with ok(i, j, pp[i], pp[j]) for all i, j,
+// by depth-first extension of consistent prefixes.
+template <class Ok, class Emit>
+void search_perms(int k, const Ok &ok, const Emit &emit) {
+  Perm pp{};
+  unsigned used = 0;
+  std::function<void(int)> go = [&](int d) {
+    if (d == k) {
+      emit(pp);
+      return;
+    }
+    for (int v = 0; v < k; ++v) {
+      if (used >> v & 1) continue;
+      bool fine = ok(d, d, v, v);
+      for (int i = 0; fine && i < d; ++i) fine = ok(i, d, pp[i], v) && ok(d, i, v, pp[i]);
+      if (!fine) continue;
+      pp[d] = v;
+      used |= 1u << v;
+      go(d + 1);
+      used &= ~(1u << v);
+    }
+  };
+  go(0);
+}
+
 // GetConditions, src/pattern.h:665-707.
 std::vector<std::pair<int, int>> symmetry_conditions(int k, std::vector<Perm> group) {
   std::vector<std::pair<int, int>> out;
@@ -120,19 +146,25 @@ int derive(HostPlan *p) {
     p->degree[i] = d;  // src/pattern.h:189-195
   }
 
-  // Both groups in one pass over all k! permutations.
-  Perm pp{};
-  std::iota(pp.begin(), pp.begin() + k, 0);
+  // Both groups by backtracking over partial permutations: a prefix
+  // pp[0..d) extends only while every pair among its vertices already obeys
+  // the relation, so the search visits the group's members and few dead ends
+  // instead of all k! permutations.  Every full permutation reached is
+  // checked once more by the whole-permutation test, and the group comes out
+  // as the same set (the conditions depend on the set only).
   std::vector<Perm> aut;
   p->multiplicity = 0;
   p->orient = 0;
-  do {
-    if (keeps_labelled_edges(*p, pp)) {
-      ++p->multiplicity;
-      if (pp[0] == 1) p->orient = 1;  // L_adj[0][1], src/pattern.h:312-340
-    }
-    if (is_automorphism(*p, pp)) aut.push_back(pp);
-  } while (std::next_permutation(pp.begin(), pp.begin() + k));
+  search_perms(k, [&](int i, int j, int pi, int pj) { return (p->adj[i][j] != 0) == (p->adj[pi][pj] == 1); },
+               [&](const Perm &pp) {
+                 if (!keeps_labelled_edges(*p, pp)) return;
+                 ++p->multiplicity;
+                 if (pp[0] == 1) p->orient = 1;  // L_adj[0][1], src/pattern.h:312-340
+               });
+  search_perms(k, [&](int i, int j, int pi, int pj) { return i == j || (p->adj[i][j] > 0) == (p->adj[pi][pj] > 0); },
+               [&](const Perm &pp) {
+                 if (is_automorphism(*p, pp)) aut.push_back(pp);
+               });
   p->conditions = symmetry_conditions(k, std::move(aut));
 
   // condition_order, src/pattern.h:416-448 (SetConditions :709-719).
