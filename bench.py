@@ -863,7 +863,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-capture", action="store_true")
     ap.add_argument("--queries", type=int, default=10000, help="c5: queries drawn for the served stream")
-    ap.add_argument("--budget", type=float, default=2e6, help="c5: device work budget per query (units)")
+    ap.add_argument("--budget", type=float, default=5e6, help="c5: device work budget per query (units)")
     ap.add_argument("--plain-sample", type=int, default=500, help="c5: queries also run as single plain launches")
     ap.add_argument("--rate", type=float, default=0.0, help="c5: Poisson arrival rate (0 = half the served capacity)")
     ap.add_argument("--inflight", type=int, default=256, help="c5: server in-flight limit")
