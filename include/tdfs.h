@@ -86,6 +86,10 @@ typedef struct {
                            its candidate set (as of its deepest backward neighbour) and reuses it
                            for every node below, cut by the conditions in between
                            (0 auto = on, -1 off) */
+  int label_rows;       /* labeled plans on a graph with at most 16 labels read only the label
+                           segment of each adjacency row they scan (rows kept a second time,
+                           sorted by label then id) (0 auto = on, -1 off: whole rows, labels
+                           tested per candidate) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

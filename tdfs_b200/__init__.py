@@ -77,6 +77,7 @@ class Options(C.Structure):
         ("leaf_steal_min", C.c_int),
         ("label_index", C.c_int),
         ("level_hoist", C.c_int),
+        ("label_rows", C.c_int),
     ]
 
 

@@ -81,6 +81,7 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.steal_first = o.steal_first > 0 ? o.steal_first : 8;
   c.leaf_min = o.leaf_steal_min > 0 ? o.leaf_steal_min : (o.leaf_steal_min < 0 ? 2 : 64);
   c.hoist = o.level_hoist < 0 ? 0 : 1;
+  c.segments = o.label_rows < 0 ? 0 : 1;
   c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 32);
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");

@@ -45,6 +45,9 @@ struct DevGraph {
   const uint8_t *label;    // n, or nullptr
   const int32_t *maxnd;    // max degree over each vertex's neighbours
   const int32_t *lperm;    // level-0 label index (labeled graphs), or nullptr
+  const int32_t *colidx_l; // labeled graphs with few labels: every row re-sorted by (label, id), or nullptr
+  const int32_t *loff;     // its segment starts: loff[v * (nlab + 1) + l], relative to rowptr[v]
+  int32_t nlab;            // labels 0..nlab-1 have segments
   int64_t nedges;
   int32_t n;
   int32_t max_degree;

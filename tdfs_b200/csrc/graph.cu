@@ -212,6 +212,30 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
         lindex->perm[(size_t)at[(size_t)(ls | lab8[(size_t)colidx[j]])]++] = (int32_t)j;
     }
   }
+  // label-partitioned rows, for graphs with at most kSegLabels labels: each
+  // row re-sorted by (label, id), a stable counting sort per row, with the
+  // start of every label's segment relative to the row start.  A labeled
+  // plan then scans only the segment of the label it needs.
+  int nlab = 0;
+  std::vector<int32_t> col_l, loff;
+  if (labels) {
+    for (int64_t v = 0; v < n; ++v) nlab = std::max(nlab, lab8[(size_t)v] + 1);
+    if (nlab > kSegLabels) nlab = 0;
+  }
+  if (nlab > 0) {
+    col_l.resize((size_t)nedges);
+    loff.assign((size_t)n * (nlab + 1), 0);
+    std::vector<int32_t> cnt(nlab + 1);
+    for (int64_t v = 0; v < n; ++v) {
+      std::fill(cnt.begin(), cnt.end(), 0);
+      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) ++cnt[lab8[(size_t)colidx[j]] + 1];
+      int32_t *o = loff.data() + (size_t)v * (nlab + 1);
+      for (int l = 0; l < nlab; ++l) o[l + 1] = o[l] + cnt[l + 1];
+      for (int l = 0; l < nlab; ++l) cnt[l] = o[l];
+      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j)
+        col_l[(size_t)(rowptr[v] + cnt[lab8[(size_t)colidx[j]]]++)] = colidx[j];
+    }
+  }
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   static_assert(kColPad % 4 == 0, "padding keeps 16-byte loads aligned");
@@ -220,7 +244,9 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   const size_t o_maxnd = o_src + align256(sizeof(int32_t) * (size_t)(nedges ? nedges : 1));
   const size_t o_label = o_maxnd + align256(sizeof(int32_t) * (size_t)(n ? n : 1));
   const size_t o_perm = o_label + align256((size_t)(labels && n ? n : 1));
-  const size_t total = o_perm + align256(sizeof(int32_t) * (size_t)(labels && nedges ? nedges : 1));
+  const size_t o_coll = o_perm + align256(sizeof(int32_t) * (size_t)(labels && nedges ? nedges : 1));
+  const size_t o_loff = o_coll + align256(sizeof(int32_t) * (size_t)(nlab ? nedges + kColPad : 1));
+  const size_t total = o_loff + align256(sizeof(int32_t) * (nlab ? loff.size() : 1));
   char *base = nullptr;
   e = cudaMalloc(&base, total);
   if (e != cudaSuccess) return cuda_fail(e, "graph arrays");
@@ -238,6 +264,9 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   g->maxnd = reinterpret_cast<int32_t *>(base + o_maxnd);
   g->label = labels ? reinterpret_cast<uint8_t *>(base + o_label) : nullptr;
   g->lperm = labels ? reinterpret_cast<int32_t *>(base + o_perm) : nullptr;
+  g->colidx_l = nlab ? reinterpret_cast<int32_t *>(base + o_coll) : nullptr;
+  g->loff = nlab ? reinterpret_cast<int32_t *>(base + o_loff) : nullptr;
+  g->nlab = nlab;
   g->bytes = total;
   const cudaStream_t st = cudaStreamPerThread;
   e = cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st);
@@ -248,6 +277,12 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
     e = cudaMemcpyAsync(g->label, lab8.data(), (size_t)n, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && labels && nedges)
     e = cudaMemcpyAsync(g->lperm, lindex->perm.data(), sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && nlab) {
+    if (nedges) e = cudaMemcpyAsync(g->colidx_l, col_l.data(), sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(g->colidx_l + nedges, 0x7f, sizeof(int32_t) * kColPad, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(g->loff, loff.data(), sizeof(int32_t) * loff.size(), cudaMemcpyHostToDevice, st);
+  }
   int rc = TDFS_OK;
   if (e == cudaSuccess && n > 0) {
     (void)cudaGetLastError();  // the check below must see these launches' errors only
@@ -303,6 +338,9 @@ DevGraph graph_view(const tdfs_graph *g) {
   v.label = g->label;
   v.maxnd = g->maxnd;
   v.lperm = g->lperm;
+  v.colidx_l = g->colidx_l;
+  v.loff = g->loff;
+  v.nlab = g->nlab;
   v.nedges = g->nedges;
   v.n = (int32_t)g->n;
   v.max_degree = g->max_degree;

@@ -12,6 +12,7 @@
 namespace tdfs {
 
 constexpr int kColPad = 256;         // int32 padding after colidx (>= merge window)
+constexpr int kSegLabels = 16;       // label-partitioned rows for graphs with at most this many labels
 constexpr int kUnitItems = 24;       // candidate vertices carried by one split unit
 constexpr int kQueueCap = 1 << 16;   // split units in the global queue
 
@@ -142,6 +143,9 @@ struct tdfs_graph {
   int32_t *maxnd;
   uint8_t *label;
   int32_t *lperm;         // device label index (labeled graphs), see LabelIndex
+  int32_t *colidx_l;      // label-partitioned rows (labeled graphs with <= kSegLabels labels)
+  int32_t *loff;          //   and their segment starts per vertex and label
+  int32_t nlab;
   tdfs::LabelIndex *lindex;  // its host copy and group offsets
   tdfs::Workspace *ws;    // launch workspace (pooled; taken at the first launch)
   tdfs::RunCtl *ctl;      // = ws->ctl etc. while a workspace is held

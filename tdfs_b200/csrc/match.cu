@@ -110,9 +110,10 @@ __device__ int32_t warp_upper_bound(const int32_t *a, int32_t lo, int32_t hi, in
 
 template <bool LAB>
 __device__ __forceinline__ bool pass_filter(int32_t x, const LevelHdr &H, int i, const DevPlan &P,
-                                            const DevGraph &G) {
+                                            const DevGraph &G, bool segmented) {
   if (LAB) {
-    if ((int32_t)G.label[x] != P.label[i]) return false;
+    // reading label segments, every source holds i's label only
+    if (!segmented && (int32_t)G.label[x] != P.label[i]) return false;
   } else {
     if (x <= H.lo || x >= H.hi) return false;
   }
@@ -214,6 +215,28 @@ struct Engine {
   __device__ __forceinline__ int32_t *buf(int l) { return bufs + (l - 2) * cfg.cap; }
   __device__ __forceinline__ int32_t *fbuf() { return win + cfg.window; }  // F (cfg.fixed)
   __device__ __forceinline__ int64_t deg(int32_t v) { return G.rowptr[v + 1] - G.rowptr[v]; }
+
+  // Adjacency rows as pattern vertex i sees them.  On a label-partitioned
+  // graph a labeled plan reads only the segment of a row that carries vertex
+  // i's label (every candidate of i must carry it); otherwise the whole row.
+  __device__ __forceinline__ bool segmented() const { return LAB && cfg.segments && G.colidx_l != nullptr; }
+  __device__ __forceinline__ const int32_t *lbase() const { return segmented() ? G.colidx_l : G.colidx; }
+  __device__ __forceinline__ void row_for(int32_t v, int i, int64_t &b, int64_t &e) const {
+    if (segmented()) {
+      const int l = P.label[i];
+      const int64_t r = G.rowptr[v];
+      if (l >= G.nlab) {  // a label no vertex carries
+        b = e = r;
+        return;
+      }
+      const int32_t *o = G.loff + (int64_t)v * (G.nlab + 1) + l;
+      b = r + o[0];
+      e = r + o[1];
+    } else {
+      b = G.rowptr[v];
+      e = G.rowptr[v + 1];
+    }
+  }
 
   // Set up the candidate scan of pattern vertex i from phi(0..i-1).
   __device__ void setup(int i, bool allow_reuse) {
@@ -364,10 +387,11 @@ struct Engine {
       nm = P.nsh[i];
       if (lane < nm) {
         const int32_t v = W.phi[P.bnsh[i][lane]];
-        const int64_t b = G.rowptr[v];
-        mylen = (int32_t)(G.rowptr[v + 1] - b);
+        int64_t b, e;
+        row_for(v, i, b, e);
+        mylen = (int32_t)(e - b);
         myslot = lane;
-        H.mlist[lane] = G.colidx + b;
+        H.mlist[lane] = lbase() + b;
         H.mlen[lane] = mylen;
         H.mcur[lane] = 0;
       }
@@ -381,8 +405,7 @@ struct Engine {
       int64_t b = 0, e = 0;
       if (part) {
         const int32_t v = W.phi[P.bn[i][lane]];
-        b = G.rowptr[v];
-        e = G.rowptr[v + 1];
+        row_for(v, i, b, e);
         key = ((unsigned long long)(e - b) << 8) | (unsigned)lane;
       }
       unsigned long long best = key;
@@ -394,14 +417,14 @@ struct Engine {
       const int bmin = (int)(best & 0xff);
       const int64_t sb = __shfl_sync(kFull, b, bmin);
       slen = (int32_t)(best >> 8);
-      src = G.colidx + sb;
+      src = lbase() + sb;
       nm = __popc(pmask) - 1;
       if (part && lane != bmin) {
         const int rank = __popc(pmask & lanemask_lt());
         const int rmin = __popc(pmask & ((1u << bmin) - 1u));
         myslot = rank < rmin ? rank : rank - 1;
         mylen = (int32_t)(e - b);
-        H.mlist[myslot] = G.colidx + b;
+        H.mlist[myslot] = lbase() + b;
         H.mlen[myslot] = mylen;
         H.mcur[myslot] = 0;
       }
@@ -470,9 +493,9 @@ struct Engine {
       const int32_t x = valid ? src[idx] : 0;
       const bool st0 = H.nm > 0 && (H.merge_mask & 1u);
       Window w0 = {0, 0};
-      if (st0) w0 = stage_window(H.mlist[0], H.mlen[0], cur[0], win, cfg.window, G.colidx);
-      bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
-      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx, st0, w0);
+      if (st0) w0 = stage_window(H.mlist[0], H.mlen[0], cur[0], win, cfg.window, lbase());
+      bool ok = valid && pass_filter<LAB>(x, H, i, P, G, segmented());
+      ok = test_lists(ok, x, H, cur, win, cfg.window, lbase(), st0, w0);
       const unsigned mask = __ballot_sync(kFull, ok);
       if (ok) out[n + __popc(mask & lanemask_lt())] = x;
       n += __popc(mask);
@@ -533,8 +556,8 @@ struct Engine {
       const int32_t idx = spos + lane;
       const bool valid = idx < send;
       const int32_t x = valid ? src[idx] : 0;
-      bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
-      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx, false, Window{0, 0});
+      bool ok = valid && pass_filter<LAB>(x, H, i, P, G, segmented());
+      ok = test_lists(ok, x, H, cur, win, cfg.window, lbase(), false, Window{0, 0});
       const unsigned mask = __ballot_sync(kFull, ok);
       if (ok) out[n + __popc(mask & lanemask_lt())] = x;
       n += __popc(mask);
@@ -600,10 +623,7 @@ struct Engine {
     if (W.fn == 0) return 0;
     const Extra X = extra_conds(i);
     int64_t b = 0, e = 0;
-    if (lane == 0) {
-      b = G.rowptr[x];
-      e = G.rowptr[x + 1];
-    }
+    if (lane == 0) row_for(x, i, b, e);
     b = __shfl_sync(kFull, b, 0);
     e = __shfl_sync(kFull, e, 0);
     return count_fixed_list(i, x, b, e, X);
@@ -633,10 +653,7 @@ struct Engine {
     const bool mine = lane < b && item_ok(i - 1, items[lane]);
     const int32_t x = mine ? items[lane] : 0;
     int64_t rb = 0, re = 0;
-    if (mine) {
-      rb = G.rowptr[x];
-      re = G.rowptr[x + 1];
-    }
+    if (mine) row_for(x, i, rb, re);
     const int64_t lim = cfg.lane_list > 4 * nF ? (int64_t)cfg.lane_list : 4ll * nF;
     const bool flat = mine && re - rb <= lim;
     const int32_t len = flat ? (int32_t)(re - rb) : 0;
@@ -667,7 +684,7 @@ struct Engine {
         const int64_t bj = __shfl_sync(kFull, rb, j);
         xo[u] = __shfl_sync(kFull, x, j);
         v[u] = pos < total;
-        y[u] = v[u] ? G.colidx[bj + (pos - oj)] : 0;
+        y[u] = v[u] ? lbase()[bj + (pos - oj)] : 0;
       }
 #pragma unroll
       for (int u = 0; u < kFlatUnroll; ++u) {
@@ -734,7 +751,7 @@ struct Engine {
   __device__ unsigned long long count_fixed_list(int i, int32_t x, int64_t b, int64_t e, const Extra &X) {
     const int32_t *F = fbuf();
     const int32_t nF = W.fn;
-    const int32_t *L = G.colidx + b;
+    const int32_t *L = lbase() + b;
     const int32_t len = (int32_t)(e - b);
     const int rel = parent_rel(i);
     unsigned long long c = 0;
@@ -822,9 +839,9 @@ struct Engine {
       const int32_t x = valid ? src[idx] : 0;
       const bool st0 = H.nm > 0 && (H.merge_mask & 1u);
       Window w0 = {0, 0};
-      if (st0) w0 = stage_window(H.mlist[0], H.mlen[0], cur[0], win, cfg.window, G.colidx);
-      bool ok = valid && pass_filter<LAB>(x, H, i, P, G);
-      ok = test_lists(ok, x, H, cur, win, cfg.window, G.colidx, st0, w0);
+      if (st0) w0 = stage_window(H.mlist[0], H.mlen[0], cur[0], win, cfg.window, lbase());
+      bool ok = valid && pass_filter<LAB>(x, H, i, P, G, segmented());
+      ok = test_lists(ok, x, H, cur, win, cfg.window, lbase(), st0, w0);
       c += __popc(__ballot_sync(kFull, ok));
     }
     return c;

@@ -65,6 +65,7 @@ struct KernelCfg {
   int32_t leaf_min;     // the last stored level (its items only count leaves) is split only
                         // with at least this many items left
   int32_t hoist;        // 1: levels whose candidates hang on an ancestor reuse a core set
+  int32_t segments;     // 1: labeled plans read the label segments of rows (DevGraph::colidx_l)
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)

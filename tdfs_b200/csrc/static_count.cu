@@ -156,6 +156,9 @@ extern "C" int tdfs_count_static(int device, int64_t n, int64_t nedges, const in
   g.label = label8;
   g.maxnd = maxnd;
   g.lperm = nullptr;  // no label index here: labeled slots walk the edge ids
+  g.colidx_l = nullptr;  // nor label-partitioned rows: labeled plans test labels per candidate
+  g.loff = nullptr;
+  g.nlab = 0;
   g.nedges = nedges;
   g.n = (int32_t)n;
   g.max_degree = 0;

@@ -35,7 +35,7 @@ OPTION_SETS = [
     {"split_rush_us": 10, "steal_first": 2},            # tail rush after 10 us
     {"split_rush_us": 1, "split_after_us": 400, "fixed_stage": -1},  # long gate, 1 us in the tail
     {"label_index": -1, "leaf_steal_min": -1},          # labeled level 0 over every edge id; leaves stealable
-    {"level_hoist": -1, "fixed_stage": -1},             # every level produced per node
+    {"level_hoist": -1, "fixed_stage": -1, "label_rows": -1},  # every level produced per node; whole rows
     {"chunk_cap": 64, "split_after_us": -1, "steal_first": 2},  # tiny buffers, eager splits of hoisted levels
 ]
 
