@@ -362,7 +362,11 @@ def run_tdfs(args, rank, world, dist):
         return o
 
     default = T.default_options()
-    tune_range = warm_r[0] if warm_r else timed_r[0]
+    # tune on the work the steps do: a whole-graph step, or -- on slice
+    # workloads, whose slices differ in cost by orders of magnitude -- the
+    # first timed slice (untimed runs, before the timed region)
+    tune_range = timed_r[0]
+    trial_ranges = (warm_r or timed_r)[:3] if slices == 1 else timed_r[:1]
     launch = {"autotune": "off"}
     knobs = default
     if not args.no_autotune:
@@ -374,7 +378,7 @@ def run_tdfs(args, rank, world, dist):
 
         def trial(o):
             ms = []
-            for r in (warm_r or timed_r)[:3]:
+            for r in trial_ranges:
                 torch.cuda.synchronize()
                 t1 = time.perf_counter()
                 T.count_batch(G, plans, shard(r, o))
@@ -382,8 +386,9 @@ def run_tdfs(args, rank, world, dist):
             return min(ms)
         d_ms, t_ms = trial(default), trial(tuned)
         knobs = tuned if t_ms <= d_ms else default
-        launch = {"autotune": "tdfs_autotune on a warm-up step (every level-0 chunk of a whole-graph step, every "
-                              "4th of a slice), kept only if faster than the defaults over warm-up steps", "autotune_s": round(tune_s, 2),
+        launch = {"autotune": "tdfs_autotune before the timed region on the step's work (every level-0 chunk of a "
+                              "whole-graph step; every 4th of the first timed slice), kept only if faster than the "
+                              "defaults there", "autotune_s": round(tune_s, 2),
                   "tuned": {f: getattr(tuned, f) for f, _ in T.Options._fields_
                             if f not in ("stream", "edge_begin", "edge_end", "edge_stride", "edge_phase")},
                   "warmup_step_ms": {"default": d_ms, "tuned": t_ms}, "chosen": "tuned" if knobs is tuned else "default"}
