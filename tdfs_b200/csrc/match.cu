@@ -25,7 +25,6 @@ constexpr int kMaxLists = kMaxK - 1;
 constexpr int kCasLimit = 1 << 20;
 constexpr int kStoredMax = kMaxK;  // level index bound (stored levels are 2..k-2)
 constexpr int kFlatUnroll = 4;     // positions per lane in flight in the flattened last-level pass
-constexpr int kSpreadSlots = 64;   // warps looking for level-0 work spread over this many open slots
 
 struct LevelHdr {
   const int32_t *src;            // source list: global adjacency list or an smem buffer
@@ -995,24 +994,14 @@ struct Engine {
       long long t = 0;
       if (lane == 0) {
         const unsigned long long adm = *(volatile unsigned long long *)&C.admitted;
-        const unsigned long long lo = *(volatile unsigned long long *)&C.first_open;
-        const unsigned long long nopen = adm > lo ? adm - lo : 0;
-        // warps spread over the oldest kSpreadSlots open slots, each starting
-        // at its own and wrapping around, so every pattern of a batch has
-        // subtrees running from the start -- the heavy ones too -- instead of
-        // the slots being drained one after another
-        const unsigned long long gw = (unsigned long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        const unsigned long long start = lo + (nopen ? gw % min(nopen, (unsigned long long)kSpreadSlots) : 0);
-        unsigned long long hint = lo;  // slots below it are known exhausted
-        for (unsigned long long i = 0; i < nopen && s < 0; ++i) {
-          unsigned long long q = start + i;
-          if (q >= adm) q -= nopen;  // wrap into [lo, adm)
+        unsigned long long lo = *(volatile unsigned long long *)&C.first_open;
+        for (unsigned long long q = lo; q < adm && s < 0; ++q) {
           SlotHot &h = tab->hot[q];
           const long long nt = __ldcg(&tab->info[q].ntickets);
           if ((long long)*(volatile unsigned long long *)&h.ticket >= nt) {
-            if (q == hint) {  // advance the hint past exhausted slots
+            if (q == lo) {  // advance the hint past exhausted slots
               atomicMax(&C.first_open, q + 1);
-              hint = q + 1;
+              lo = q + 1;
             }
             continue;
           }
