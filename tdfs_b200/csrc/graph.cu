@@ -18,6 +18,7 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "csr.h"
@@ -168,74 +169,231 @@ void release_workspace(tdfs_graph *g) {
   std::lock_guard<std::mutex> lk(g_pool_mu);
   int idle = 0;
   for (Workspace *x : g_pool) idle += x->device == w->device;
-  if (idle < kIdlePerDevice) g_pool.push_back(w);
+  if (idle < kIdlePerDevice) g_pool.insert(g_pool.end(), 1, w);
   else free_workspace(w);
 }
 
 }  // namespace
 
-// The graph arrays live in one device allocation:
-//   rowptr int64[n+1] | colidx int32[E + kColPad] | src int32[E] | maxnd int32[n] | label uint8[n]
-// each part starting on a 256-byte boundary.  Labels are checked and
-// narrowed to 8 bits on the host, so the upload is a few stream-ordered
-// copies and two preprocessing kernels, synchronised once at the end.
+namespace {
+
+// ---- cached allocations ----------------------------------------------------
+// A freed graph's device block and pinned staging block are kept for the next
+// upload, so a create/free cycle of a small graph pays no cudaMalloc,
+// cudaMallocHost or cudaFree (each costs more than the rest of its upload).
+class BlockCache {
+ public:
+  BlockCache(bool pinned, size_t cap) : pinned_(pinned), cap_(cap) {}
+
+  // A block of at least `need` bytes for `device` (the current device):
+  // the smallest idle one within twice that, else a new allocation (after
+  // returning this device's idle blocks when memory is short).
+  cudaError_t take(int device, size_t need, void **p, size_t *bytes) {
+    need = (need + kGrain - 1) & ~(kGrain - 1);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      int best = -1;
+      for (size_t i = 0; i < idle_.size(); ++i) {
+        const Block &b = idle_[i];
+        if (b.device == device && b.bytes >= need && b.bytes <= 2 * need &&
+            (best < 0 || b.bytes < idle_[(size_t)best].bytes))
+          best = (int)i;
+      }
+      if (best >= 0) {
+        *p = idle_[(size_t)best].p;
+        *bytes = idle_[(size_t)best].bytes;
+        idle_bytes_ -= *bytes;
+        idle_.erase(idle_.begin() + best);
+        return cudaSuccess;
+      }
+    }
+    cudaError_t e = alloc(p, need);
+    if (e == cudaErrorMemoryAllocation) {
+      (void)cudaGetLastError();
+      drop(device);
+      e = alloc(p, need);
+    }
+    if (e == cudaSuccess) *bytes = need;
+    return e;
+  }
+
+  // Keep a block for reuse (within the cache's byte cap), else free it.
+  void give(int device, void *p, size_t bytes) {
+    if (!p) return;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      int mine = 0;
+      for (const Block &b : idle_) mine += b.device == device;
+      if (idle_bytes_ + bytes <= cap_ && mine < kPerDevice) {
+        idle_.push_back(Block{device, bytes, p});
+        idle_bytes_ += bytes;
+        return;
+      }
+    }
+    release(p);
+  }
+
+ private:
+  struct Block {
+    int device;
+    size_t bytes;
+    void *p;
+  };
+  static constexpr size_t kGrain = size_t(1) << 20;  // sizes rounded to 1 MiB, so re-uploads fit exactly
+  static constexpr int kPerDevice = 4;
+
+  cudaError_t alloc(void **p, size_t bytes) { return pinned_ ? cudaMallocHost(p, bytes) : cudaMalloc(p, bytes); }
+  void release(void *p) {
+    if (pinned_) cudaFreeHost(p); else cudaFree(p);
+  }
+  void drop(int device) {
+    std::vector<Block> mine;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (size_t i = 0; i < idle_.size();) {
+        if (idle_[i].device == device) {
+          idle_bytes_ -= idle_[i].bytes;
+          mine.push_back(idle_[i]);
+          idle_.erase(idle_.begin() + (long)i);
+        } else {
+          ++i;
+        }
+      }
+    }
+    for (const Block &b : mine) release(b.p);
+  }
+
+  std::mutex mu_;
+  std::vector<Block> idle_;
+  size_t idle_bytes_ = 0;
+  const bool pinned_;
+  const size_t cap_;
+};
+
+// never destroyed: the blocks may outlive the CUDA runtime at process exit
+BlockCache &device_blocks() {
+  static BlockCache *c = new BlockCache(false, size_t(512) << 20);
+  return *c;
+}
+BlockCache &pinned_blocks() {
+  static BlockCache *c = new BlockCache(true, size_t(256) << 20);
+  return *c;
+}
+
+int host_threads() {
+  const unsigned t = std::thread::hardware_concurrency();
+  return t ? (int)std::min(t, 32u) : 4;
+}
+
+// The label index and the label rows, written by the host straight into the
+// pinned staging block they are uploaded from:
+//  * perm: a stable counting sort of the edge ids by the group key
+//    nl * label(src) + label(dst), with its group offsets `off`;
+//  * with nlab > 0 (at most kSegLabels labels, nlab == nl): col_l, every row
+//    re-sorted by (label, id), and loff, each row's segment starts relative
+//    to the row start (nlab + 1 per vertex).
+// Two passes over the edges (count, then scatter).  Large graphs split the
+// rows over host threads in contiguous runs of about equal edge counts; each
+// run scatters from its own group offsets, so the order stays stable.
+void build_label_arrays(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx, const uint8_t *lab,
+                        int nl, int nlab, int32_t *perm, int32_t *col_l, int32_t *loff, std::vector<int64_t> &off) {
+  const int G = nl * nl;
+  const int T = nedges < (int64_t(1) << 20) ? 1 : (int)std::min<int64_t>(host_threads(), nedges >> 19);
+  std::vector<int64_t> rb((size_t)T + 1, 0);
+  rb[(size_t)T] = n;
+  for (int t = 1; t < T; ++t) {
+    const int64_t want = nedges * t / T;
+    rb[(size_t)t] = std::max(rb[(size_t)t - 1], (int64_t)(std::upper_bound(rowptr, rowptr + n + 1, want) - rowptr) - 1);
+  }
+  std::vector<int64_t> cnt((size_t)T * G, 0);  // per run and group: edges, then the run's scatter cursor
+  auto count_run = [&](int t) {
+    int64_t *c = cnt.data() + (size_t)t * G;
+    for (int64_t v = rb[(size_t)t]; v < rb[(size_t)t + 1]; ++v) {
+      int64_t *cv = c + (size_t)lab[v] * nl;
+      if (nlab) {
+        int32_t k[kSegLabels] = {0};
+        for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) ++k[lab[colidx[j]]];
+        int32_t *o = loff + (size_t)v * (nlab + 1);
+        o[0] = 0;
+        for (int l = 0; l < nlab; ++l) {
+          o[l + 1] = o[l] + k[l];
+          cv[l] += k[l];
+        }
+      } else {
+        for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) ++cv[lab[colidx[j]]];
+      }
+    }
+  };
+  auto scatter_run = [&](int t) {
+    int64_t *at = cnt.data() + (size_t)t * G;
+    for (int64_t v = rb[(size_t)t]; v < rb[(size_t)t + 1]; ++v) {
+      int64_t *av = at + (size_t)lab[v] * nl;
+      const int64_t b = rowptr[v], e = rowptr[v + 1];
+      if (nlab) {
+        int32_t k[kSegLabels];
+        const int32_t *o = loff + (size_t)v * (nlab + 1);
+        for (int l = 0; l < nlab; ++l) k[l] = o[l];
+        for (int64_t j = b; j < e; ++j) {
+          const int32_t x = colidx[j];
+          const int l = lab[x];
+          perm[av[l]++] = (int32_t)j;
+          col_l[b + k[l]++] = x;
+        }
+      } else {
+        for (int64_t j = b; j < e; ++j) perm[av[lab[colidx[j]]]++] = (int32_t)j;
+      }
+    }
+  };
+  auto run = [&](auto &&f) {
+    if (T == 1) {
+      f(0);
+      return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; ++t) th.emplace_back(f, t);
+    for (auto &x : th) x.join();
+  };
+  run(count_run);
+  off.assign((size_t)G + 1, 0);
+  for (int gk = 0; gk < G; ++gk) {
+    int64_t s = off[(size_t)gk];
+    for (int t = 0; t < T; ++t) {  // run t scatters group gk from here
+      const int64_t c = cnt[(size_t)t * G + gk];
+      cnt[(size_t)t * G + gk] = s;
+      s += c;
+    }
+    off[(size_t)gk + 1] = s;
+  }
+  run(scatter_run);
+}
+
+}  // namespace
+
+// The graph arrays live in one device allocation, each part starting on a
+// 256-byte boundary:
+//   rowptr int64[n+1] | colidx int32[E + kColPad] | src int32[E] | maxnd int32[n]
+//   | label uint8[n] | lperm int32[E] | colidx_l int32[E + kColPad] | loff int32[n (nlab+1)]
+// The parts from `label` on are derived on the host into one pinned staging
+// block laid out the same way and uploaded with one copy.  The CSR copies and
+// the two preprocessing kernels are queued first, so the device works while
+// the host sorts; one synchronisation at the end.
 int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t *colidx, const int32_t *labels,
                  int device, int32_t max_degree, tdfs_graph **out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return fail(TDFS_ERR_CUDA, "no CUDA device visible (the tdfs engine has no CPU path)");
   if (device < 0 || device >= ndev) return fail(TDFS_ERR_ARG, "device %d out of range", device);
-  std::vector<uint8_t> lab8;
-  std::unique_ptr<LabelIndex> lindex;
+  int nl = 0;
   if (labels) {
-    lab8.resize((size_t)n);
     for (int64_t i = 0; i < n; ++i) {
       if (labels[i] < 0 || labels[i] > 254)
         return fail(TDFS_ERR_FORMAT, "vertex labels must lie in [0, 254] for the device label array");
-      lab8[(size_t)i] = (uint8_t)labels[i];
+      nl = std::max(nl, labels[i] + 1);
     }
-    // level-0 label index: a stable counting sort of the edge ids by
-    // (label(src), label(dst))
-    lindex.reset(new LabelIndex);
-    std::vector<int64_t> &off = lindex->off;
-    off.assign(65537, 0);
-    for (int64_t v = 0; v < n; ++v) {
-      const int ls = lab8[(size_t)v] << 8;
-      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) ++off[(size_t)(ls | lab8[(size_t)colidx[j]]) + 1];
-    }
-    for (size_t k = 1; k < off.size(); ++k) off[k] += off[k - 1];
-    std::vector<int64_t> at(off.begin(), off.end() - 1);
-    lindex->perm.resize((size_t)nedges);
-    for (int64_t v = 0; v < n; ++v) {
-      const int ls = lab8[(size_t)v] << 8;
-      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j)
-        lindex->perm[(size_t)at[(size_t)(ls | lab8[(size_t)colidx[j]])]++] = (int32_t)j;
-    }
+    if (nedges > INT32_MAX) return fail(TDFS_ERR_CAPACITY, "labeled graphs hold at most 2^31 - 1 directed edges");
   }
-  // label-partitioned rows, for graphs with at most kSegLabels labels: each
-  // row re-sorted by (label, id), a stable counting sort per row, with the
-  // start of every label's segment relative to the row start.  A labeled
-  // plan then scans only the segment of the label it needs.
-  int nlab = 0;
-  std::vector<int32_t> col_l, loff;
-  if (labels) {
-    for (int64_t v = 0; v < n; ++v) nlab = std::max(nlab, lab8[(size_t)v] + 1);
-    if (nlab > kSegLabels) nlab = 0;
-  }
-  if (nlab > 0) {
-    col_l.resize((size_t)nedges);
-    loff.assign((size_t)n * (nlab + 1), 0);
-    std::vector<int32_t> cnt(nlab + 1);
-    for (int64_t v = 0; v < n; ++v) {
-      std::fill(cnt.begin(), cnt.end(), 0);
-      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j) ++cnt[lab8[(size_t)colidx[j]] + 1];
-      int32_t *o = loff.data() + (size_t)v * (nlab + 1);
-      for (int l = 0; l < nlab; ++l) o[l + 1] = o[l] + cnt[l + 1];
-      for (int l = 0; l < nlab; ++l) cnt[l] = o[l];
-      for (int64_t j = rowptr[v]; j < rowptr[v + 1]; ++j)
-        col_l[(size_t)(rowptr[v] + cnt[lab8[(size_t)colidx[j]]]++)] = colidx[j];
-    }
-  }
+  // label-partitioned rows for graphs with at most kSegLabels labels
+  const int nlab = labels && nl <= kSegLabels ? nl : 0;
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
   static_assert(kColPad % 4 == 0, "padding keeps 16-byte loads aligned");
@@ -246,10 +404,20 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   const size_t o_perm = o_label + align256((size_t)(labels && n ? n : 1));
   const size_t o_coll = o_perm + align256(sizeof(int32_t) * (size_t)(labels && nedges ? nedges : 1));
   const size_t o_loff = o_coll + align256(sizeof(int32_t) * (size_t)(nlab ? nedges + kColPad : 1));
-  const size_t total = o_loff + align256(sizeof(int32_t) * (nlab ? loff.size() : 1));
-  char *base = nullptr;
-  e = cudaMalloc(&base, total);
+  const size_t nloff = nlab ? (size_t)n * (size_t)(nlab + 1) : 0;
+  const size_t total = o_loff + align256(sizeof(int32_t) * (nloff ? nloff : 1));
+  void *arrays = nullptr, *stage = nullptr;
+  size_t array_bytes = 0, stage_bytes = 0;
+  e = device_blocks().take(device, total, &arrays, &array_bytes);
   if (e != cudaSuccess) return cuda_fail(e, "graph arrays");
+  if (labels) {
+    e = pinned_blocks().take(device, total - o_label, &stage, &stage_bytes);
+    if (e != cudaSuccess) {
+      device_blocks().give(device, arrays, array_bytes);
+      return cuda_fail(e, "pinned staging for the label arrays");
+    }
+  }
+  char *base = static_cast<char *>(arrays);
   auto *g = new tdfs_graph;
   std::memset(g, 0, sizeof *g);
   g->device = device;
@@ -257,7 +425,10 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   g->nedges = nedges;
   g->max_degree = max_degree;
   g->labeled = labels != nullptr;
-  g->arrays = base;
+  g->arrays = arrays;
+  g->array_bytes = array_bytes;
+  g->staging = stage;
+  g->staging_bytes = stage_bytes;
   g->rowptr = reinterpret_cast<int64_t *>(base);
   g->colidx = reinterpret_cast<int32_t *>(base + o_col);
   g->src = reinterpret_cast<int32_t *>(base + o_src);
@@ -273,17 +444,6 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   if (e == cudaSuccess && nedges)
     e = cudaMemcpyAsync(g->colidx, colidx, sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(g->colidx + nedges, 0x7f, sizeof(int32_t) * kColPad, st);
-  if (e == cudaSuccess && labels && n)
-    e = cudaMemcpyAsync(g->label, lab8.data(), (size_t)n, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && labels && nedges)
-    e = cudaMemcpyAsync(g->lperm, lindex->perm.data(), sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && nlab) {
-    if (nedges) e = cudaMemcpyAsync(g->colidx_l, col_l.data(), sizeof(int32_t) * nedges, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(g->colidx_l + nedges, 0x7f, sizeof(int32_t) * kColPad, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(g->loff, loff.data(), sizeof(int32_t) * loff.size(), cudaMemcpyHostToDevice, st);
-  }
-  int rc = TDFS_OK;
   if (e == cudaSuccess && n > 0) {
     (void)cudaGetLastError();  // the check below must see these launches' errors only
     const int threads = 256;
@@ -293,11 +453,29 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
     max_nbr_deg_kernel<<<blocks, threads, 0, st>>>(g->rowptr, g->colidx, (int32_t)n, g->maxnd);
     e = cudaGetLastError();
   }
-  // the host label copy and the caller's arrays must outlive the copies
+  std::unique_ptr<LabelIndex> lindex;
+  if (e == cudaSuccess && labels) {
+    // while the device copies and preprocesses the CSR
+    char *h = static_cast<char *>(stage);
+    auto *lab8 = reinterpret_cast<uint8_t *>(h);
+    for (int64_t i = 0; i < n; ++i) lab8[i] = (uint8_t)labels[i];
+    auto *perm = reinterpret_cast<int32_t *>(h + (o_perm - o_label));
+    auto *col_l = reinterpret_cast<int32_t *>(h + (o_coll - o_label));
+    auto *loff = reinterpret_cast<int32_t *>(h + (o_loff - o_label));
+    lindex.reset(new LabelIndex);
+    lindex->nl = nl;
+    lindex->perm = perm;
+    build_label_arrays(n, nedges, rowptr, colidx, lab8, nl, nlab, perm, col_l, loff, lindex->off);
+    if (nlab) std::memset(col_l + nedges, 0x7f, sizeof(int32_t) * kColPad);
+    e = cudaMemcpyAsync(base + o_label, h, total - o_label, cudaMemcpyHostToDevice, st);
+  }
+  // the staging block and the caller's arrays must outlive the copies
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) rc = cuda_fail(e, "graph upload");
-  if (rc) {
-    cudaFree(base);
+  if (e != cudaSuccess) {
+    const int rc = cuda_fail(e, "graph upload");
+    cudaStreamSynchronize(st);
+    pinned_blocks().give(device, stage, stage_bytes);
+    device_blocks().give(device, arrays, array_bytes);
     delete g;
     return rc;
   }
@@ -308,9 +486,9 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
 
 void label_range(const LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e) {
   *b = *e = 0;
-  if (l0 < 0 || l0 > 254 || l1 < 0 || l1 > 254) return;  // a label no vertex has: nothing to do
-  const size_t key = (size_t)(l0 << 8 | l1);
-  const int32_t *g0 = x.perm.data() + x.off[key], *g1 = x.perm.data() + x.off[key + 1];
+  if (l0 < 0 || l0 >= x.nl || l1 < 0 || l1 >= x.nl) return;  // a label no vertex has: nothing to do
+  const size_t key = (size_t)l0 * (size_t)x.nl + (size_t)l1;
+  const int32_t *g0 = x.perm + x.off[key], *g1 = x.perm + x.off[key + 1];
   // ids ascend within a group: the edge-id range is a position range
   *b = x.off[key] + (std::lower_bound(g0, g1, (int32_t)std::min<int64_t>(eb, INT32_MAX)) - g0);
   *e = x.off[key] + (std::lower_bound(g0, g1, (int32_t)std::min<int64_t>(ee, INT32_MAX)) - g0);
@@ -324,7 +502,11 @@ void graph_release(tdfs_graph *g) {
   cudaSetDevice(g->device);
   release_graphs(g);
   release_workspace(g);
-  cudaFree(g->arrays);
+  // the blocks go back to the caches, not to the driver: wait for anything
+  // still reading them, as cudaFree would
+  cudaDeviceSynchronize();
+  device_blocks().give(g->device, g->arrays, g->array_bytes);
+  pinned_blocks().give(g->device, g->staging, g->staging_bytes);
   delete g->lindex;
   cudaSetDevice(cur);
   delete g;

@@ -121,8 +121,9 @@ namespace tdfs {
 // A labeled plan's level-0 tickets run over its group only, so none of them is
 // spent on edges the label test would drop.
 struct LabelIndex {
-  std::vector<int32_t> perm;  // host copy of the device array
-  std::vector<int64_t> off;   // group of key = 256 * l0 + l1 is perm[off[key], off[key + 1])
+  const int32_t *perm = nullptr;  // host copy of the device array (in the graph's pinned staging block)
+  std::vector<int64_t> off;       // group of key = nl * l0 + l1 is perm[off[key], off[key + 1])
+  int nl = 0;                     // labels of the graph lie in [0, nl)
 };
 
 // Group range of plan labels (l0, l1) restricted to edge ids [eb, ee).
@@ -147,6 +148,9 @@ struct tdfs_graph {
   int32_t *loff;          //   and their segment starts per vertex and label
   int32_t nlab;
   tdfs::LabelIndex *lindex;  // its host copy and group offsets
+  size_t array_bytes;     // size of the `arrays` block (cached for reuse when the graph is freed)
+  void *staging;          // pinned host block: the derived arrays as uploaded (labeled graphs)
+  size_t staging_bytes;
   tdfs::Workspace *ws;    // launch workspace (pooled; taken at the first launch)
   tdfs::RunCtl *ctl;      // = ws->ctl etc. while a workspace is held
   tdfs::SplitUnit *queue;
