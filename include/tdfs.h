@@ -90,6 +90,11 @@ typedef struct {
                            segment of each adjacency row they scan (rows kept a second time,
                            sorted by label then id) (0 auto = on, -1 off: whole rows, labels
                            tested per candidate) */
+  int tail_count;       /* when the last 2 or 3 pattern vertices hang only on vertices up to some
+                           level s (no edge among them, and on unlabeled plans no order condition
+                           between them), a node at level s counts the leaves below it as the
+                           tuples of distinct vertices from their candidate sets, by
+                           inclusion-exclusion, instead of enumerating them (0 auto = on, -1 off) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

@@ -78,6 +78,7 @@ class Options(C.Structure):
         ("label_index", C.c_int),
         ("level_hoist", C.c_int),
         ("label_rows", C.c_int),
+        ("tail_count", C.c_int),
     ]
 
 

@@ -55,13 +55,14 @@ struct alignas(16) WarpSmem {
   int32_t fvalid;                // 0: stale, 1: F holds the fixed set, 2: too large
   int32_t fn;                    // |F|
   int32_t xneq[kMaxK];           // values the last vertex must differ from, between F's anchor and the parent
+  int32_t tn[3];                 // count_tail: sizes of the tail's candidate sets
   // derived from the plan once per plan switch (derive_plan)
   int8_t hanchor[kMaxK];         // per level: anchor of a hoisted level, -1 when not hoisted
   uint8_t hneq[kMaxK];           // per hoisted level: bit j = candidates must differ from phi(j)
   int8_t fanchor;                // anchor of the last vertex's fixed set
   int8_t lastmode;               // last vertex: 2 parent-free fixed set, 1 fixed set with the parent, 0 neither
   uint8_t hoistmask;             // bit i: level i is hoisted
-  int8_t pad_d_;
+  int8_t tail;                   // level whose nodes count their independent tail in closed form, -1 none
   unsigned long long t_base;     // globaltimer when the current base work was taken
   // lane 0's bookkeeping, kept here rather than in registers every lane holds
   unsigned long long idle_since; // bounded idle wait: start of the current wait
@@ -300,8 +301,33 @@ struct Engine {
       const int last = P.k - 1;
       W.fanchor = (int8_t)fixed_anchor(last);
       W.lastmode = (int8_t)(free_applies(last) ? 2 : fixed_applies(last) ? 1 : 0);
+      W.tail = (int8_t)tail_level();
     }
     __syncwarp();
+  }
+
+  // ---- independent tail ------------------------------------------------------
+  // The last t = k-1-s pattern vertices (2 <= t <= 3, s >= 2) form an
+  // independent tail when every backward neighbour of each lies at or above
+  // level s, and -- on unlabeled plans -- no order condition ties two of them.
+  // Below a node at level s their candidate sets A_j are then fixed (the
+  // backward neighbours' lists, filtered by the conditions on phi(0..s)), and
+  // the leaves the DFS would count are exactly the tuples of distinct
+  // vertices drawn one from each set; count_tail counts them by
+  // inclusion-exclusion instead of enumerating levels s+1..k-1.  The smallest
+  // such s is taken.  Returns s, or -1.
+  __device__ int tail_level() const {
+    if (!cfg.tail || !cfg.fixed) return -1;
+    const int k = P.k;
+    for (int s = max(2, k - 4); s <= k - 3; ++s) {
+      bool ok = true;
+      for (int j = s + 1; j < k; ++j) {
+        for (int t = 0; t < P.nbn[j]; ++t) ok &= P.bn[j][t] <= s;
+        if (!LAB) ok &= ((unsigned)(P.larger[j] | P.less[j]) >> (s + 1)) == 0;
+      }
+      if (ok) return s;
+    }
+    return -1;
   }
 
   // Lane-wise: may candidate x of level l be claimed under the current
@@ -536,10 +562,12 @@ struct Engine {
     return has_parent;
   }
 
-  __device__ void build_fixed(int i) {
+  // Scan vertex i's candidates under the backward neighbours and conditions
+  // of the vertices up to `limit` into `out` (scratch header W.hf).  Returns
+  // their number, or -1 when they might not fit in `cap` entries.
+  __device__ int32_t collect(int i, int limit, int32_t *out) {
     LevelHdr &H = W.hf;
-    setup_into(H, i, false, W.fanchor);
-    int32_t *out = fbuf();
+    setup_into(H, i, false, limit);
     const int32_t *src = H.src;
     const int32_t send = H.send;
     int32_t cur[kMaxLists];
@@ -563,11 +591,80 @@ struct Engine {
       n += __popc(mask);
     }
     __syncwarp();
+    return over ? -1 : n;
+  }
+
+  __device__ void build_fixed(int i) {
+    const int32_t n = collect(i, W.fanchor, fbuf());
     if (lane == 0) {
-      W.fn = n;
-      W.fvalid = over ? 2 : 1;
+      W.fn = max(n, 0);
+      W.fvalid = n < 0 ? 2 : 1;
     }
     __syncwarp();
+  }
+
+  // |a ∩ b| of two sorted sets in shared memory (lanes search the smaller
+  // one's elements in the larger); with c, |a ∩ b ∩ c|.
+  __device__ int32_t common_count(const int32_t *a, int32_t na, const int32_t *b, int32_t nb,
+                                  const int32_t *c = nullptr, int32_t nc = 0) {
+    if (na > nb) {
+      const int32_t *t = a; a = b; b = t;
+      const int32_t u = na; na = nb; nb = u;
+    }
+    int32_t r = 0;
+    for (int32_t pos = 0; pos < na; pos += 32) {
+      const int32_t idx = pos + lane;
+      bool ok = idx < na;
+      if (ok) {
+        const int32_t y = a[idx];
+        const int32_t q = lower_bound(b, 0, nb, y);
+        ok = q < nb && b[q] == y;
+        if (ok && c) {
+          const int32_t q2 = lower_bound(c, 0, nc, y);
+          ok = q2 < nc && c[q2] == y;
+        }
+      }
+      r += __popc(__ballot_sync(kFull, ok));
+    }
+    return r;
+  }
+
+  // Leaves below the current node at level s = W.tail: the tuples of
+  // distinct vertices from the tail's candidate sets A_{s+1}, .., A_{k-1},
+  // built into the buffers of levels s+1.. and F's buffer.  With t = 2:
+  // |A||B| - |A ∩ B|; with t = 3: |A||B||C| - |A ∩ B||C| - |A ∩ C||B|
+  // - |B ∩ C||A| + 2|A ∩ B ∩ C|.  On labeled plans two tail vertices with
+  // different labels never meet, so their intersection term is dropped.
+  // Returns -1 when a set might not fit its buffer; the caller then descends
+  // the ordinary way (the buffers' previous contents are marked stale here).
+  __device__ long long count_tail(int s) {
+    const int k = P.k;
+    const int t = k - 1 - s;
+    if (lane == 0) {
+      W.fvalid = 0;
+      for (int l = s + 1; l <= k - 2; ++l) W.h[l].core = W.h[l].complete = 0;
+    }
+    __syncwarp();
+    // one call site of collect for the t sets (the kernel's code stays small)
+#pragma unroll 1
+    for (int u = 0; u < t; ++u) {
+      const int32_t n = collect(s + 1 + u, s, u == t - 1 ? fbuf() : buf(s + 1 + u));
+      if (n <= 0) return n;  // -1: might not fit; 0: an empty set, no leaves
+      if (lane == 0) W.tn[u] = n;
+    }
+    __syncwarp();
+    const int32_t *A0 = buf(s + 1), *A1 = t == 2 ? fbuf() : buf(s + 2), *A2 = fbuf();
+    const int32_t n0 = W.tn[0], n1 = W.tn[1], n2 = t == 3 ? W.tn[2] : 1;
+    const bool e01 = !LAB || P.label[s + 1] == P.label[s + 2];
+    long long c = (long long)n0 * n1 * n2;
+    if (e01) c -= (long long)common_count(A0, n0, A1, n1) * n2;
+    if (t == 2) return c;
+    const bool e02 = !LAB || P.label[s + 1] == P.label[s + 3];
+    const bool e12 = !LAB || P.label[s + 2] == P.label[s + 3];
+    if (e02) c -= (long long)common_count(A0, n0, A2, n2) * n1;
+    if (e12) c -= (long long)common_count(A1, n1, A2, n2) * n0;
+    if (e01 && e02) c += 2ll * common_count(A0, n0, A1, n1, A2, n2);
+    return c;
   }
 
   // Conditions of the last vertex i on the vertices between F's anchor and
@@ -1492,6 +1589,13 @@ struct Engine {
             continue;
           }
           if (cfg.steal) maybe_donate(level);
+        }
+        if (level == W.tail) {
+          const long long c = count_tail(level);
+          if (c >= 0) {
+            count += (unsigned long long)c;
+            continue;
+          }
         }
         if (level + 1 == P.k - 1) {
           count += count_last(P.k - 1);
