@@ -174,17 +174,54 @@ def step_ranges(nedges, slices, steps, warmup):
 
 
 class ClockSampler:
-    """nvidia-smi SM clock / throttle-reason sampler (200 ms period)."""
+    """SM clock and throttle reasons sampled during the timed region: through
+    NVML every millisecond in a thread (a timed region of a few milliseconds
+    still gets samples), else nvidia-smi at its 200 ms period.  The GPU is
+    found by the CUDA device's UUID, so a remapped CUDA_VISIBLE_DEVICES
+    still samples the device the bench runs on.  Read-only: no setting of the
+    GPU is touched."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, device_index):
         self.dev = device_index
         self.rows = []
         self.proc = None
+        self.nvml = None
+        self.stop_flag = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+        h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        bits = [pynvml.nvmlClocksEventReasonHwSlowdown, pynvml.nvmlClocksEventReasonHwThermalSlowdown,
+                pynvml.nvmlClocksEventReasonSwThermalSlowdown, pynvml.nvmlClocksEventReasonSwPowerCap]
+        return pynvml, h, bits
+
+    def _nvml_loop(self):
+        nv, h, bits = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                clk = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(clk), [n for n, b in zip(self.NAMES, bits) if r & b]))
+            except Exception:  # noqa: BLE001 -- a failed read is a missing sample
+                pass
+            time.sleep(0.001)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.max_mhz = float(self.nvml[0].nvmlDeviceGetMaxClockInfo(self.nvml[1], self.nvml[0].NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:  # noqa: BLE001 -- no NVML: nvidia-smi below
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -199,6 +236,13 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self):
+        if self.nvml:
+            self.stop_flag.set()
+            self.thread.join(timeout=10)
+            sm = [c for c, _ in self.rows]
+            reasons = sorted({n for _, rs in self.rows for n in rs})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(sm), "sampled": "NVML, every 1 ms during the timed region"}
         if not self.proc:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -213,12 +257,11 @@ class ClockSampler:
             except (OSError, subprocess.SubprocessError):
                 pass
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in self.rows:
             try:
                 sm.append(float(r[1]))
                 mx = float(r[2])
-                for n, v in zip(names, r[5:9]):
+                for n, v in zip(self.NAMES, r[5:9]):
                     if v.lower().startswith("active"):
                         reasons.add(n)
             except (ValueError, IndexError):

@@ -172,7 +172,9 @@ int tdfs_selftest_wait_limit(tdfs_graph *g, int wait_limit_ms, float *kernel_ms)
  * t % sample_stride == 0) by coordinate descent over warps per CTA, candidate
  * chunk depth, the steal threshold, stealing on/off, the merge window and the
  * merge/search switch point, and returns the fastest as *best (base's edge
- * range and stream kept).  *best_ms = its sample time. */
+ * range and stream kept).  *best_ms = its sample time.  Under a work budget
+ * (base->work_budget) the score is the sample time per completed plan, so a
+ * shape that abandons plans early does not win by it. */
 int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *base,
                   int sample_stride, tdfs_options *best, float *best_ms);
 

@@ -535,14 +535,19 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
   cur.edge_phase = 0;
   std::vector<uint64_t> counts(nplans);
   std::vector<int> status(nplans);
+  // the score is the sample's kernel time per completed plan, scaled to the
+  // batch: the plain time when every plan completes; under a work budget a
+  // shape that completes more plans in the same time scores better (a plan
+  // abandoned early is cheap, but it is not an answer)
   auto measure = [&](const tdfs_options &o, float *out) -> int {
     float bestt = 1e30f;
     for (int rep = 0; rep < 2; ++rep) {
       float ms = 0.f;
-      // a plan that runs out of a work budget is timed like the others
       int rc = tdfs_count_batch_status(g, plans, nplans, &o, counts.data(), status.data(), &ms);
       if (rc) return rc;
-      bestt = std::min(bestt, ms);
+      int done = 0;
+      for (int i = 0; i < nplans; ++i) done += status[i] == TDFS_OK;
+      bestt = std::min(bestt, ms * (float)nplans / (float)std::max(1, done));
     }
     *out = bestt;
     return TDFS_OK;

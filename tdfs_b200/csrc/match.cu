@@ -60,7 +60,8 @@ struct alignas(16) WarpSmem {
   int8_t hanchor[kMaxK];         // per level: anchor of a hoisted level, -1 when not hoisted
   uint8_t hneq[kMaxK];           // per hoisted level: bit j = candidates must differ from phi(j)
   int8_t fanchor;                // anchor of the last vertex's fixed set
-  int8_t lastmode;               // last vertex: 2 parent-free fixed set, 1 fixed set with the parent, 0 neither
+  int8_t lastmode;               // last vertex: 2 parent-free fixed set, 1 fixed set with the parent,
+                                 // 3 the parent its one backward neighbour (label segments), 0 none of these
   uint8_t hoistmask;             // bit i: level i is hoisted
   int8_t tail;                   // level whose nodes count their independent tail in closed form, -1 none
   unsigned long long t_base;     // globaltimer when the current base work was taken
@@ -300,7 +301,7 @@ struct Engine {
       W.hoistmask = (uint8_t)hm;
       const int last = P.k - 1;
       W.fanchor = (int8_t)fixed_anchor(last);
-      W.lastmode = (int8_t)(free_applies(last) ? 2 : fixed_applies(last) ? 1 : 0);
+      W.lastmode = (int8_t)(free_applies(last) ? 2 : fixed_applies(last) ? 1 : single_applies(last) ? 3 : 0);
       W.tail = (int8_t)tail_level();
     }
     __syncwarp();
@@ -810,6 +811,38 @@ struct Engine {
   // injectivity when labeled).  F is sorted, so sibling x counts a range of
   // F by two binary searches in shared memory, less the excluded values that
   // fall in it; lane j takes sibling j.
+  // Last vertex i whose one backward neighbour is its parent, on a labeled
+  // plan reading label segments: sibling x's candidates are the label-L(i)
+  // segment of N(x) minus the prefix vertices, so each sibling's count is a
+  // segment length and a few searches (count_single_batch).
+  __device__ bool single_applies(int i) {
+    return LAB && segmented() && i >= 3 && P.nbn[i] == 1 && P.bn[i][0] == i - 1;
+  }
+
+  // Lane t counts sibling t of the batch: the length of the label-L(i)
+  // segment of N(x), minus the vertices of phi(0..i-2) and x itself (the
+  // values the labeled DFS excludes) that carry that label and are found in
+  // the segment by binary search.
+  __device__ unsigned long long count_single_batch(int i, const int32_t *items, int b) {
+    unsigned c = 0;
+    if (lane < b && item_ok(i - 1, items[lane])) {
+      const int32_t x = items[lane];
+      int64_t rb, re;
+      row_for(x, i, rb, re);
+      const int32_t *L = lbase() + rb;
+      const int32_t len = (int32_t)(re - rb);
+      int32_t cnt = len;
+      for (int j = 0; j < i; ++j) {
+        const int32_t v = j < i - 1 ? W.phi[j] : x;
+        if ((int32_t)G.label[v] != P.label[i]) continue;  // not in this segment
+        const int32_t q = lower_bound(L, 0, len, v);
+        if (q < len && L[q] == v) --cnt;
+      }
+      c = (unsigned)cnt;
+    }
+    return __reduce_add_sync(kFull, c);
+  }
+
   __device__ bool free_applies(int i) {
     if (!cfg.fixed || i < 3) return false;
     for (int t = 0; t < P.nbn[i]; ++t)
@@ -1544,10 +1577,12 @@ struct Engine {
         // last stored level: batches of up to 32 siblings against the fixed
         // part of the last vertex's candidates (built once per grandparent)
         const int i = level + 1;
-        const int mode = W.lastmode == 2 ? 2 : (cfg.lane_list > 0 && W.lastmode == 1) ? 1 : 0;
+        const int lm = W.lastmode;
+        // (mode 3 exists on labeled plans only: kept out of the unlabeled kernel)
+        const int mode = lm == 2 ? 2 : (cfg.lane_list > 0 && (lm == 1 || (LAB && lm == 3))) ? lm : 0;
         if (mode) {
-          if (W.fvalid == 0) build_fixed(i);
-          if (W.fvalid == 1) {
+          if (mode != 3 && W.fvalid == 0) build_fixed(i);
+          if (mode == 3 || W.fvalid == 1) {
             int b = 0;
             const int32_t first = claim_batch(level, &b);
             if (b > 0) {
@@ -1557,8 +1592,9 @@ struct Engine {
                 level = base - 1;
                 continue;
               }
-              count += mode == 2 ? count_free_batch(i, buf(level) + first, b)
-                                 : count_fixed_flat(i, buf(level) + first, b);
+              count += mode == 2           ? count_free_batch(i, buf(level) + first, b)
+                       : (!LAB || mode == 1) ? count_fixed_flat(i, buf(level) + first, b)
+                                             : count_single_batch(i, buf(level) + first, b);
               if (cfg.steal && (cfg.budgeted ? (claims & 7u) == 0 : (++claims & 7u) == 0)) maybe_donate(level);
               continue;
             }
