@@ -142,8 +142,8 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
 void level0_range(const tdfs_graph *g, const DevPlan &p, int64_t eb, int64_t ee, bool use_index, SlotInfo *in) {
   ee = std::max(eb, ee);
   in->perm = 0;
-  if (use_index && p.labeled && g->lindex) {
-    label_range(*g->lindex, p.label[0], p.label[1], eb, ee, &in->e_begin, &in->e_end);
+  if (use_index && p.labeled && g->lindex &&
+      label_range(*g->lindex, p.label[0], p.label[1], eb, ee, &in->e_begin, &in->e_end)) {
     in->perm = 1;
     return;
   }

@@ -64,6 +64,157 @@ __global__ void narrow_labels_kernel(const int32_t *__restrict__ in, int32_t n, 
   }
 }
 
+__device__ __forceinline__ unsigned lanes_below() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// ---- label rows and label index on the device (at most kSegLabels labels) --
+// Both are stable counting sorts.  Within a warp, the lanes holding the same
+// key are found with __match_any_sync; each lane's rank among them (lanes
+// below it) plus the counts of the earlier chunks gives its position, so the
+// output keeps the input order within every key, as a sequential pass would.
+
+constexpr int kTileEdges = 4096;  // edge ids per tile of the label-index sort
+constexpr int kBuildWarps = 8;    // warps per CTA of the build kernels
+
+// One warp per vertex: its row again, stably partitioned by neighbour label
+// (col_l), and each label's segment start relative to the row start (loff,
+// nl + 1 per vertex, the last one the row length).  Two passes over the row:
+// the label counts, then the scatter.
+__global__ void label_rows_kernel(const int64_t *__restrict__ rowptr, const int32_t *__restrict__ colidx,
+                                  const uint8_t *__restrict__ lab, int32_t n, int nl, int32_t *__restrict__ col_l,
+                                  int32_t *__restrict__ loff) {
+  __shared__ int32_t cnt_s[kBuildWarps][kSegLabels];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int32_t *cnt = cnt_s[wib];
+  const int64_t warps = (int64_t)gridDim.x * kBuildWarps;
+  for (int64_t v = (int64_t)blockIdx.x * kBuildWarps + wib; v < n; v += warps) {
+    const int64_t b = rowptr[v], e = rowptr[v + 1];
+    if (lane < kSegLabels) cnt[lane] = 0;
+    __syncwarp();
+    for (int64_t c0 = b; c0 < e; c0 += 32) {
+      const int64_t j = c0 + lane;
+      const bool valid = j < e;
+      const int key = valid ? (int)lab[colidx[j]] : -1;
+      const unsigned m = __match_any_sync(0xffffffffu, key);
+      if (valid && lane == __ffs(m) - 1) cnt[key] += __popc(m);
+      __syncwarp();
+    }
+    const int32_t c = lane < nl ? cnt[lane] : 0;
+    int32_t incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+      if (lane >= d) incl += t;
+    }
+    const int32_t excl = incl - c;  // lane nl: the row length
+    if (lane <= nl) loff[v * (nl + 1) + lane] = excl;
+    __syncwarp();
+    if (lane < nl) cnt[lane] = excl;  // scatter cursors
+    __syncwarp();
+    for (int64_t c0 = b; c0 < e; c0 += 32) {
+      const int64_t j = c0 + lane;
+      const bool valid = j < e;
+      const int32_t w = valid ? colidx[j] : 0;
+      const int key = valid ? (int)lab[w] : -1;
+      const unsigned m = __match_any_sync(0xffffffffu, key);
+      if (valid) col_l[b + cnt[key] + __popc(m & lanes_below())] = w;
+      __syncwarp();
+      if (valid && lane == __ffs(m) - 1) cnt[key] += __popc(m);
+      __syncwarp();
+    }
+  }
+}
+
+// One warp per tile of kTileEdges consecutive edge ids: the number of the
+// tile's edges with each group key nl * label(src) + label(dst), written
+// key-major (hist[key * ntiles + tile]) so that one exclusive scan gives every
+// (key, tile) its first position in the label index.
+__global__ void edge_hist_kernel(const int32_t *__restrict__ src, const int32_t *__restrict__ colidx,
+                                 const uint8_t *__restrict__ lab, int64_t nedges, int nl, int32_t ntiles,
+                                 int32_t *__restrict__ hist) {
+  __shared__ int32_t cnt_s[kBuildWarps][kSegLabels * kSegLabels];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int32_t *cnt = cnt_s[wib];
+  const int G = nl * nl;
+  const int64_t warps = (int64_t)gridDim.x * kBuildWarps;
+  for (int64_t t = (int64_t)blockIdx.x * kBuildWarps + wib; t < ntiles; t += warps) {
+    for (int k = lane; k < G; k += 32) cnt[k] = 0;
+    __syncwarp();
+    const int64_t b = t * kTileEdges, e = b + kTileEdges < nedges ? b + kTileEdges : nedges;
+    for (int64_t c0 = b; c0 < e; c0 += 32) {
+      const int64_t j = c0 + lane;
+      const bool valid = j < e;
+      const int key = valid ? (int)lab[src[j]] * nl + (int)lab[colidx[j]] : -1;
+      const unsigned m = __match_any_sync(0xffffffffu, key);
+      if (valid && lane == __ffs(m) - 1) cnt[key] += __popc(m);
+      __syncwarp();
+    }
+    for (int k = lane; k < G; k += 32) hist[(int64_t)k * ntiles + t] = cnt[k];
+    __syncwarp();
+  }
+}
+
+// One CTA of 1024 threads: exclusive scan of the histogram in place (each
+// thread a contiguous run, then a scan of the run sums in shared memory), and
+// the group offsets goff[key] (goff[G] = the edge count).
+__global__ void __launch_bounds__(1024) index_scan_kernel(int32_t *__restrict__ a, int64_t N, int G,
+                                                          int32_t ntiles, int64_t nedges,
+                                                          int64_t *__restrict__ goff) {
+  __shared__ int64_t part[1024];
+  const int t = threadIdx.x;
+  const int64_t per = (N + 1023) / 1024;
+  const int64_t b = t * per < N ? t * per : N, e = b + per < N ? b + per : N;
+  int64_t s = 0;
+  for (int64_t i = b; i < e; ++i) s += a[i];
+  part[t] = s;
+  __syncthreads();
+  for (int d = 1; d < 1024; d <<= 1) {
+    const int64_t v = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  int64_t run = part[t] - s;
+  for (int64_t i = b; i < e; ++i) {
+    const int32_t x = a[i];
+    a[i] = (int32_t)run;
+    run += x;
+  }
+  __syncthreads();
+  for (int k = t; k < G; k += 1024) goff[k] = a[(int64_t)k * ntiles];
+  if (t == 0) goff[G] = nedges;
+}
+
+// One warp per tile: every edge id to its place in the label index, from the
+// scanned (key, tile) starts, in edge-id order within each key.
+__global__ void edge_scatter_kernel(const int32_t *__restrict__ src, const int32_t *__restrict__ colidx,
+                                    const uint8_t *__restrict__ lab, int64_t nedges, int nl, int32_t ntiles,
+                                    const int32_t *__restrict__ start, int32_t *__restrict__ perm) {
+  __shared__ int32_t cur_s[kBuildWarps][kSegLabels * kSegLabels];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int32_t *cur = cur_s[wib];
+  const int G = nl * nl;
+  const int64_t warps = (int64_t)gridDim.x * kBuildWarps;
+  for (int64_t t = (int64_t)blockIdx.x * kBuildWarps + wib; t < ntiles; t += warps) {
+    for (int k = lane; k < G; k += 32) cur[k] = start[(int64_t)k * ntiles + t];
+    __syncwarp();
+    const int64_t b = t * kTileEdges, e = b + kTileEdges < nedges ? b + kTileEdges : nedges;
+    for (int64_t c0 = b; c0 < e; c0 += 32) {
+      const int64_t j = c0 + lane;
+      const bool valid = j < e;
+      const int key = valid ? (int)lab[src[j]] * nl + (int)lab[colidx[j]] : -1;
+      const unsigned m = __match_any_sync(0xffffffffu, key);
+      if (valid) perm[cur[key] + __popc(m & lanes_below())] = (int32_t)j;
+      __syncwarp();
+      if (valid && lane == __ffs(m) - 1) cur[key] += __popc(m);
+      __syncwarp();
+    }
+  }
+}
+
 // Report a failed CUDA call and clear the runtime's last-error slot, so the
 // error cannot resurface in a later launch check.
 int cuda_fail(cudaError_t e, const char *what) {
@@ -405,13 +556,22 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   const size_t o_coll = o_perm + align256(sizeof(int32_t) * (size_t)(labels && nedges ? nedges : 1));
   const size_t o_loff = o_coll + align256(sizeof(int32_t) * (size_t)(nlab ? nedges + kColPad : 1));
   const size_t nloff = nlab ? (size_t)n * (size_t)(nlab + 1) : 0;
-  const size_t total = o_loff + align256(sizeof(int32_t) * (nloff ? nloff : 1));
+  // with label rows the label arrays are built on the device, which needs
+  // scratch for the index sort: the (key, tile) histogram and the group
+  // offsets; otherwise the host builds them into the staging block
+  const bool dev_build = nlab > 0;
+  const int G = nl * nl;
+  const int32_t ntiles = dev_build ? (int32_t)((nedges + kTileEdges - 1) / kTileEdges) : 0;
+  const size_t o_hist = o_loff + align256(sizeof(int32_t) * (nloff ? nloff : 1));
+  const size_t o_goff = o_hist + align256(sizeof(int32_t) * (size_t)(dev_build && ntiles ? (int64_t)G * ntiles : 1));
+  const size_t total = dev_build ? o_goff + align256(sizeof(int64_t) * (size_t)(G + 1)) : o_hist;
   void *arrays = nullptr, *stage = nullptr;
   size_t array_bytes = 0, stage_bytes = 0;
   e = device_blocks().take(device, total, &arrays, &array_bytes);
   if (e != cudaSuccess) return cuda_fail(e, "graph arrays");
   if (labels) {
-    e = pinned_blocks().take(device, total - o_label, &stage, &stage_bytes);
+    e = pinned_blocks().take(device, dev_build ? (size_t)std::max<int64_t>(n, 1) : total - o_label, &stage,
+                             &stage_bytes);
     if (e != cudaSuccess) {
       device_blocks().give(device, arrays, array_bytes);
       return cuda_fail(e, "pinned staging for the label arrays");
@@ -438,7 +598,7 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   g->colidx_l = nlab ? reinterpret_cast<int32_t *>(base + o_coll) : nullptr;
   g->loff = nlab ? reinterpret_cast<int32_t *>(base + o_loff) : nullptr;
   g->nlab = nlab;
-  g->bytes = total;
+  g->bytes = dev_build ? o_hist : total;  // the scratch is not part of the graph
   const cudaStream_t st = cudaStreamPerThread;
   e = cudaMemcpyAsync(g->rowptr, rowptr, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && nedges)
@@ -455,19 +615,49 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   }
   std::unique_ptr<LabelIndex> lindex;
   if (e == cudaSuccess && labels) {
-    // while the device copies and preprocesses the CSR
     char *h = static_cast<char *>(stage);
     auto *lab8 = reinterpret_cast<uint8_t *>(h);
     for (int64_t i = 0; i < n; ++i) lab8[i] = (uint8_t)labels[i];
-    auto *perm = reinterpret_cast<int32_t *>(h + (o_perm - o_label));
-    auto *col_l = reinterpret_cast<int32_t *>(h + (o_coll - o_label));
-    auto *loff = reinterpret_cast<int32_t *>(h + (o_loff - o_label));
     lindex.reset(new LabelIndex);
     lindex->nl = nl;
-    lindex->perm = perm;
-    build_label_arrays(n, nedges, rowptr, colidx, lab8, nl, nlab, perm, col_l, loff, lindex->off);
-    if (nlab) std::memset(col_l + nedges, 0x7f, sizeof(int32_t) * kColPad);
-    e = cudaMemcpyAsync(base + o_label, h, total - o_label, cudaMemcpyHostToDevice, st);
+    lindex->nedges = nedges;
+    if (dev_build) {
+      // label rows and label index by the kernels above, after the CSR's
+      // preprocessing in stream order; the host keeps the group offsets
+      lindex->dev_perm = g->lperm;
+      lindex->off.assign((size_t)G + 1, 0);
+      e = cudaMemcpyAsync(g->label, lab8, (size_t)n, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaMemsetAsync(g->colidx_l + nedges, 0x7f, sizeof(int32_t) * kColPad, st);
+      if (e == cudaSuccess && n > 0) {
+        const int blocks = (int)std::min<int64_t>((n + kBuildWarps - 1) / kBuildWarps, 148 * 16);
+        label_rows_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->rowptr, g->colidx, g->label, (int32_t)n, nl,
+                                                              g->colidx_l, g->loff);
+        e = cudaGetLastError();
+      }
+      if (e == cudaSuccess && ntiles > 0) {
+        auto *hist = reinterpret_cast<int32_t *>(base + o_hist);
+        auto *goff = reinterpret_cast<int64_t *>(base + o_goff);
+        const int blocks = (int)std::min<int64_t>((ntiles + kBuildWarps - 1) / kBuildWarps, 148 * 16);
+        edge_hist_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->src, g->colidx, g->label, nedges, nl, ntiles,
+                                                             hist);
+        index_scan_kernel<<<1, 1024, 0, st>>>(hist, (int64_t)G * ntiles, G, ntiles, nedges, goff);
+        edge_scatter_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->src, g->colidx, g->label, nedges, nl, ntiles,
+                                                                hist, g->lperm);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+          e = cudaMemcpyAsync(lindex->off.data(), goff, sizeof(int64_t) * (size_t)(G + 1), cudaMemcpyDeviceToHost,
+                              st);
+      }
+    } else {
+      // while the device copies and preprocesses the CSR
+      auto *perm = reinterpret_cast<int32_t *>(h + (o_perm - o_label));
+      auto *col_l = reinterpret_cast<int32_t *>(h + (o_coll - o_label));
+      auto *loff = reinterpret_cast<int32_t *>(h + (o_loff - o_label));
+      lindex->perm = perm;
+      build_label_arrays(n, nedges, rowptr, colidx, lab8, nl, nlab, perm, col_l, loff, lindex->off);
+      if (nlab) std::memset(col_l + nedges, 0x7f, sizeof(int32_t) * kColPad);
+      e = cudaMemcpyAsync(base + o_label, h, total - o_label, cudaMemcpyHostToDevice, st);
+    }
   }
   // the staging block and the caller's arrays must outlive the copies
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -484,15 +674,31 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   return TDFS_OK;
 }
 
-void label_range(const LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e) {
+bool label_range(LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e) {
   *b = *e = 0;
-  if (l0 < 0 || l0 >= x.nl || l1 < 0 || l1 >= x.nl) return;  // a label no vertex has: nothing to do
+  if (l0 < 0 || l0 >= x.nl || l1 < 0 || l1 >= x.nl) return true;  // a label no vertex has: nothing to do
   const size_t key = (size_t)l0 * (size_t)x.nl + (size_t)l1;
+  if (eb <= 0 && ee >= x.nedges) {
+    *b = x.off[key];
+    *e = x.off[key + 1];
+    return true;
+  }
+  std::call_once(x.fetch_once, [&x] {
+    if (x.perm || !x.dev_perm) return;
+    x.fetched.resize((size_t)x.nedges);
+    if (cudaMemcpy(x.fetched.data(), x.dev_perm, sizeof(int32_t) * (size_t)x.nedges, cudaMemcpyDeviceToHost) ==
+        cudaSuccess)
+      x.perm = x.fetched.data();
+    else
+      (void)cudaGetLastError();
+  });
+  if (!x.perm) return false;
   const int32_t *g0 = x.perm + x.off[key], *g1 = x.perm + x.off[key + 1];
   // ids ascend within a group: the edge-id range is a position range
   *b = x.off[key] + (std::lower_bound(g0, g1, (int32_t)std::min<int64_t>(eb, INT32_MAX)) - g0);
   *e = x.off[key] + (std::lower_bound(g0, g1, (int32_t)std::min<int64_t>(ee, INT32_MAX)) - g0);
   if (ee > INT32_MAX) *e = x.off[key + 1];
+  return true;
 }
 
 void graph_release(tdfs_graph *g) {

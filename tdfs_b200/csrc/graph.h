@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.h"
@@ -121,13 +122,23 @@ namespace tdfs {
 // A labeled plan's level-0 tickets run over its group only, so none of them is
 // spent on edges the label test would drop.
 struct LabelIndex {
-  const int32_t *perm = nullptr;  // host copy of the device array (in the graph's pinned staging block)
   std::vector<int64_t> off;       // group of key = nl * l0 + l1 is perm[off[key], off[key + 1])
   int nl = 0;                     // labels of the graph lie in [0, nl)
+  int64_t nedges = 0;
+  // host copy of the sorted edge ids: written by the host build (in the
+  // graph's pinned staging block), or fetched from the device array at the
+  // first launch over part of the edge ids (a whole-range launch needs only off)
+  const int32_t *perm = nullptr;
+  const int32_t *dev_perm = nullptr;
+  std::vector<int32_t> fetched;
+  std::once_flag fetch_once;
 };
 
 // Group range of plan labels (l0, l1) restricted to edge ids [eb, ee).
-void label_range(const LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e);
+// False when the host copy of the index could not be fetched (the caller
+// then walks every edge id of the range instead).  The graph's device must be
+// current.
+bool label_range(LabelIndex &x, int l0, int l1, int64_t eb, int64_t ee, int64_t *b, int64_t *e);
 
 }  // namespace tdfs
 
