@@ -95,6 +95,9 @@ typedef struct {
                            between them), a node at level s counts the leaves below it as the
                            tuples of distinct vertices from their candidate sets, by
                            inclusion-exclusion, instead of enumerating them (0 auto = on, -1 off) */
+  int dead_prune;       /* a node at level a is not descended when a later pattern vertex whose
+                           backward neighbours all lie at or above a has no candidate under the
+                           conditions so far: no leaf can lie below it (0 auto = on, -1 off) */
 } tdfs_options;
 
 const char *tdfs_last_error(void);

@@ -79,6 +79,7 @@ class Options(C.Structure):
         ("level_hoist", C.c_int),
         ("label_rows", C.c_int),
         ("tail_count", C.c_int),
+        ("dead_prune", C.c_int),
     ]
 
 

@@ -83,6 +83,7 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   c.hoist = o.level_hoist < 0 ? 0 : 1;
   c.segments = o.label_rows < 0 ? 0 : 1;
   c.tail = o.tail_count < 0 ? 0 : 1;
+  c.prune = o.dead_prune < 0 ? 0 : 1;
   c.lane_list = o.lane_list > 0 ? o.lane_list : (o.lane_list < 0 ? 0 : 32);
   c.merge_ratio = o.merge_ratio > 0 ? o.merge_ratio : 4;
   if (c.steal_min < 2 || c.steal_min > 4096) return fail(TDFS_ERR_ARG, "steal_min must lie in [2, 4096]");
@@ -531,6 +532,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
   if (cur.steal_min <= 0) cur.steal_min = 2;
   if (cur.merge_ratio <= 0) cur.merge_ratio = 4;
   if (cur.tail_count == 0) cur.tail_count = 1;
+  if (cur.dead_prune == 0) cur.dead_prune = 1;
   cur.edge_stride = sample_stride;
   cur.edge_phase = 0;
   std::vector<uint64_t> counts(nplans);
@@ -577,6 +579,7 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
       {&tdfs_options::leaf_steal_min, {-1, 16, 64, 256}},
       {&tdfs_options::level_hoist, {-1, 1}},
       {&tdfs_options::tail_count, {-1, 1}},
+      {&tdfs_options::dead_prune, {-1, 1}},
   };
   for (const Knob &k : knobs) {
     for (int v : k.values) {

@@ -76,7 +76,15 @@ __device__ __forceinline__ unsigned lanes_below() {
 // below it) plus the counts of the earlier chunks gives its position, so the
 // output keeps the input order within every key, as a sequential pass would.
 
-constexpr int kTileEdges = 4096;  // edge ids per tile of the label-index sort
+// Edge ids per tile of the label-index sort: small tiles for parallelism
+// (one warp walks a tile in order), at most kMaxTiles of them so the
+// (key, tile) histogram stays a few MB.
+constexpr int64_t kMinTileEdges = 512;
+constexpr int64_t kMaxTiles = 8192;
+inline int64_t tile_edges(int64_t nedges) {
+  const int64_t t = (nedges + kMaxTiles - 1) / kMaxTiles;
+  return std::max(kMinTileEdges, (t + 31) & ~int64_t(31));
+}
 constexpr int kBuildWarps = 8;    // warps per CTA of the build kernels
 
 // One warp per vertex: its row again, stably partitioned by neighbour label
@@ -128,13 +136,13 @@ __global__ void label_rows_kernel(const int64_t *__restrict__ rowptr, const int3
   }
 }
 
-// One warp per tile of kTileEdges consecutive edge ids: the number of the
+// One warp per tile of `tile` consecutive edge ids: the number of the
 // tile's edges with each group key nl * label(src) + label(dst), written
 // key-major (hist[key * ntiles + tile]) so that one exclusive scan gives every
 // (key, tile) its first position in the label index.
 __global__ void edge_hist_kernel(const int32_t *__restrict__ src, const int32_t *__restrict__ colidx,
-                                 const uint8_t *__restrict__ lab, int64_t nedges, int nl, int32_t ntiles,
-                                 int32_t *__restrict__ hist) {
+                                 const uint8_t *__restrict__ lab, int64_t nedges, int64_t tile, int nl,
+                                 int32_t ntiles, int32_t *__restrict__ hist) {
   __shared__ int32_t cnt_s[kBuildWarps][kSegLabels * kSegLabels];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   int32_t *cnt = cnt_s[wib];
@@ -143,7 +151,7 @@ __global__ void edge_hist_kernel(const int32_t *__restrict__ src, const int32_t 
   for (int64_t t = (int64_t)blockIdx.x * kBuildWarps + wib; t < ntiles; t += warps) {
     for (int k = lane; k < G; k += 32) cnt[k] = 0;
     __syncwarp();
-    const int64_t b = t * kTileEdges, e = b + kTileEdges < nedges ? b + kTileEdges : nedges;
+    const int64_t b = t * tile, e = b + tile < nedges ? b + tile : nedges;
     for (int64_t c0 = b; c0 < e; c0 += 32) {
       const int64_t j = c0 + lane;
       const bool valid = j < e;
@@ -191,8 +199,9 @@ __global__ void __launch_bounds__(1024) index_scan_kernel(int32_t *__restrict__ 
 // One warp per tile: every edge id to its place in the label index, from the
 // scanned (key, tile) starts, in edge-id order within each key.
 __global__ void edge_scatter_kernel(const int32_t *__restrict__ src, const int32_t *__restrict__ colidx,
-                                    const uint8_t *__restrict__ lab, int64_t nedges, int nl, int32_t ntiles,
-                                    const int32_t *__restrict__ start, int32_t *__restrict__ perm) {
+                                    const uint8_t *__restrict__ lab, int64_t nedges, int64_t tile, int nl,
+                                    int32_t ntiles, const int32_t *__restrict__ start,
+                                    int32_t *__restrict__ perm) {
   __shared__ int32_t cur_s[kBuildWarps][kSegLabels * kSegLabels];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   int32_t *cur = cur_s[wib];
@@ -201,7 +210,7 @@ __global__ void edge_scatter_kernel(const int32_t *__restrict__ src, const int32
   for (int64_t t = (int64_t)blockIdx.x * kBuildWarps + wib; t < ntiles; t += warps) {
     for (int k = lane; k < G; k += 32) cur[k] = start[(int64_t)k * ntiles + t];
     __syncwarp();
-    const int64_t b = t * kTileEdges, e = b + kTileEdges < nedges ? b + kTileEdges : nedges;
+    const int64_t b = t * tile, e = b + tile < nedges ? b + tile : nedges;
     for (int64_t c0 = b; c0 < e; c0 += 32) {
       const int64_t j = c0 + lane;
       const bool valid = j < e;
@@ -561,7 +570,8 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
   // offsets; otherwise the host builds them into the staging block
   const bool dev_build = nlab > 0;
   const int G = nl * nl;
-  const int32_t ntiles = dev_build ? (int32_t)((nedges + kTileEdges - 1) / kTileEdges) : 0;
+  const int64_t tile = tile_edges(nedges);
+  const int32_t ntiles = dev_build ? (int32_t)((nedges + tile - 1) / tile) : 0;
   const size_t o_hist = o_loff + align256(sizeof(int32_t) * (nloff ? nloff : 1));
   const size_t o_goff = o_hist + align256(sizeof(int32_t) * (size_t)(dev_build && ntiles ? (int64_t)G * ntiles : 1));
   const size_t total = dev_build ? o_goff + align256(sizeof(int64_t) * (size_t)(G + 1)) : o_hist;
@@ -638,11 +648,11 @@ int graph_upload(int64_t n, int64_t nedges, const int64_t *rowptr, const int32_t
         auto *hist = reinterpret_cast<int32_t *>(base + o_hist);
         auto *goff = reinterpret_cast<int64_t *>(base + o_goff);
         const int blocks = (int)std::min<int64_t>((ntiles + kBuildWarps - 1) / kBuildWarps, 148 * 16);
-        edge_hist_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->src, g->colidx, g->label, nedges, nl, ntiles,
-                                                             hist);
+        edge_hist_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->src, g->colidx, g->label, nedges, tile, nl,
+                                                             ntiles, hist);
         index_scan_kernel<<<1, 1024, 0, st>>>(hist, (int64_t)G * ntiles, G, ntiles, nedges, goff);
-        edge_scatter_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->src, g->colidx, g->label, nedges, nl, ntiles,
-                                                                hist, g->lperm);
+        edge_scatter_kernel<<<blocks, 32 * kBuildWarps, 0, st>>>(g->src, g->colidx, g->label, nedges, tile, nl,
+                                                                ntiles, hist, g->lperm);
         e = cudaGetLastError();
         if (e == cudaSuccess)
           e = cudaMemcpyAsync(lindex->off.data(), goff, sizeof(int64_t) * (size_t)(G + 1), cudaMemcpyDeviceToHost,

@@ -64,6 +64,8 @@ struct alignas(16) WarpSmem {
                                  // 3 the parent its one backward neighbour (label segments), 0 none of these
   uint8_t hoistmask;             // bit i: level i is hoisted
   int8_t tail;                   // level whose nodes count their independent tail in closed form, -1 none
+  uint8_t deadmask[kMaxK];       // per level a: bit j = vertex j's candidates depend on phi(0..a) only and
+                                 // are checked for emptiness at each level-a node (dead-subtree pruning)
   unsigned long long t_base;     // globaltimer when the current base work was taken
   // lane 0's bookkeeping, kept here rather than in registers every lane holds
   unsigned long long idle_since; // bounded idle wait: start of the current wait
@@ -303,8 +305,32 @@ struct Engine {
       W.fanchor = (int8_t)fixed_anchor(last);
       W.lastmode = (int8_t)(free_applies(last) ? 2 : fixed_applies(last) ? 1 : single_applies(last) ? 3 : 0);
       W.tail = (int8_t)tail_level();
+      for (int a = 0; a < kMaxK; ++a) W.deadmask[a] = 0;
+      if (LAB && cfg.prune) {  // labeled plans: sparse label sets make empty ones common
+        for (int j = 3; j < P.k; ++j) {
+          int a = 1;  // level-1 items set phi(0) and phi(1) together
+          for (int t = 0; t < P.nbn[j]; ++t) a = max(a, (int)P.bn[j][t]);
+          if (j >= a + 2) W.deadmask[a] |= (uint8_t)(1u << j);
+        }
+      }
     }
     __syncwarp();
+  }
+
+  // ---- dead subtrees ---------------------------------------------------------
+  // A vertex j whose backward neighbours all lie at or above level a < j-1
+  // has, below a node at level a, candidates that are a subset of its
+  // backward neighbours' lists filtered by the conditions on phi(0..a).  When
+  // that set is empty, no node below has a leaf: the node is not descended.
+  // The check scans only until its first candidate.
+  __device__ bool subtree_dead(int a) {
+    unsigned m = W.deadmask[a];
+    while (m) {
+      const int j = __ffs(m) - 1;
+      m &= m - 1;
+      if (collect(j, a, nullptr) == 0) return true;
+    }
+    return false;
   }
 
   // ---- independent tail ------------------------------------------------------
@@ -565,7 +591,9 @@ struct Engine {
 
   // Scan vertex i's candidates under the backward neighbours and conditions
   // of the vertices up to `limit` into `out` (scratch header W.hf).  Returns
-  // their number, or -1 when they might not fit in `cap` entries.
+  // their number, or -1 when they might not fit in `cap` entries.  With
+  // out == nullptr nothing is stored and the scan stops at the first
+  // candidate (the result is then 0 or more).
   __device__ int32_t collect(int i, int limit, int32_t *out) {
     LevelHdr &H = W.hf;
     setup_into(H, i, false, limit);
@@ -578,7 +606,7 @@ struct Engine {
     bool over = false;
     for (int32_t spos = H.spos; spos < send; spos += 32) {
       ++work;
-      if (n > cfg.cap - 32) {  // a full step could write past the buffer: give up
+      if (out && n > cfg.cap - 32) {  // a full step could write past the buffer: give up
         over = true;
         break;
       }
@@ -588,8 +616,9 @@ struct Engine {
       bool ok = valid && pass_filter<LAB>(x, H, i, P, G, segmented());
       ok = test_lists(ok, x, H, cur, win, cfg.window, lbase(), false, Window{0, 0});
       const unsigned mask = __ballot_sync(kFull, ok);
-      if (ok) out[n + __popc(mask & lanemask_lt())] = x;
+      if (ok && out) out[n + __popc(mask & lanemask_lt())] = x;
       n += __popc(mask);
+      if (!out && n > 0) break;
     }
     __syncwarp();
     return over ? -1 : n;
@@ -1635,6 +1664,8 @@ struct Engine {
         }
         if (level + 1 == P.k - 1) {
           count += count_last(P.k - 1);
+        } else if (LAB && W.deadmask[level] && subtree_dead(level)) {
+          continue;  // no leaf below this node
         } else {
           const int i = level + 1;
           const int a = hoist_anchor(i);

@@ -67,6 +67,7 @@ struct KernelCfg {
   int32_t hoist;        // 1: levels whose candidates hang on an ancestor reuse a core set
   int32_t segments;     // 1: labeled plans read the label segments of rows (DevGraph::colidx_l)
   int32_t tail;         // 1: nodes above an independent tail count it in closed form (count_tail)
+  int32_t prune;        // 1: nodes whose subtree must be empty are not descended (subtree_dead)
 };
 
 constexpr int kEdgeChunk = 32;  // largest level-0 ticket (one edge per lane)

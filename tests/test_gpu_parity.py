@@ -37,7 +37,7 @@ OPTION_SETS = [
     {"label_index": -1, "leaf_steal_min": -1},          # labeled level 0 over every edge id; leaves stealable
     {"level_hoist": -1, "fixed_stage": -1, "label_rows": -1},  # every level produced per node; whole rows
     {"chunk_cap": 64, "split_after_us": -1, "steal_first": 2},  # tiny buffers, eager splits of hoisted levels
-    {"tail_count": -1, "lane_list": -1},  # independent tails enumerated like any other level
+    {"tail_count": -1, "lane_list": -1, "dead_prune": -1},  # every level enumerated, no dead-subtree checks
 ]
 
 
@@ -123,7 +123,7 @@ def test_powerlaw_labeled_random(cl):
         cl.check(random_pattern(4 + t % 4, 0.45, 4, rng), True)
 
 
-@pytest.mark.parametrize("opt", [{}, {"chunk_cap": 64}, {"tail_count": -1}])
+@pytest.mark.parametrize("opt", [{}, {"chunk_cap": 64}, {"tail_count": -1}, {"dead_prune": -1}])
 def test_independent_tails(er, cl_small, T, opt):
     """Patterns whose last two or three vertices hang only on earlier ones and
     not on each other: a node at the root of that tail counts its leaves by
