@@ -55,7 +55,8 @@ struct alignas(16) WarpSmem {
   int32_t fvalid;                // 0: stale, 1: F holds the fixed set, 2: too large
   int32_t fn;                    // |F|
   int32_t xneq[kMaxK];           // values the last vertex must differ from, between F's anchor and the parent
-  int32_t tn[3];                 // count_tail: sizes of the tail's candidate sets
+  int32_t tn[3];                 // count_tail: sizes of the tail's base sets
+  int8_t tanc[4];                //   and the level each base's conditions reach
   // derived from the plan once per plan switch (derive_plan)
   int8_t hanchor[kMaxK];         // per level: anchor of a hoisted level, -1 when not hoisted
   uint8_t hneq[kMaxK];           // per hoisted level: bit j = candidates must differ from phi(j)
@@ -667,7 +668,9 @@ struct Engine {
   // different labels never meet, so their intersection term is dropped.
   // Returns -1 when a set might not fit its buffer; the caller then descends
   // the ordinary way (the buffers' previous contents are marked stale here).
-  __device__ long long count_tail(int s) {
+  // Unlabeled plans: every tail set built per node, with the conditions on
+  // phi(0..s) (order conditions included), so no base needs a correction.
+  __device__ long long count_tail_per_node(int s) {
     const int k = P.k;
     const int t = k - 1 - s;
     if (lane == 0) {
@@ -675,7 +678,6 @@ struct Engine {
       for (int l = s + 1; l <= k - 2; ++l) W.h[l].core = W.h[l].complete = 0;
     }
     __syncwarp();
-    // one call site of collect for the t sets (the kernel's code stays small)
 #pragma unroll 1
     for (int u = 0; u < t; ++u) {
       const int32_t n = collect(s + 1 + u, s, u == t - 1 ? fbuf() : buf(s + 1 + u));
@@ -685,15 +687,108 @@ struct Engine {
     __syncwarp();
     const int32_t *A0 = buf(s + 1), *A1 = t == 2 ? fbuf() : buf(s + 2), *A2 = fbuf();
     const int32_t n0 = W.tn[0], n1 = W.tn[1], n2 = t == 3 ? W.tn[2] : 1;
-    const bool e01 = !LAB || P.label[s + 1] == P.label[s + 2];
-    long long c = (long long)n0 * n1 * n2;
-    if (e01) c -= (long long)common_count(A0, n0, A1, n1) * n2;
+    long long c = (long long)n0 * n1 * n2 - (long long)common_count(A0, n0, A1, n1) * n2;
     if (t == 2) return c;
+    c -= (long long)common_count(A0, n0, A2, n2) * n1;
+    c -= (long long)common_count(A1, n1, A2, n2) * n0;
+    c += 2ll * common_count(A0, n0, A1, n1, A2, n2);
+    return c;
+  }
+
+  __device__ long long count_tail(int s) {
+    if (!LAB) return count_tail_per_node(s);
+    const int k = P.k;
+    const int t = k - 1 - s;
+    // phi(s) just changed: the sets anchored at s or deeper are stale
+    stale_from(s);
+    // Each tail set is taken from a base that may be shared by all nodes
+    // below an earlier level: a hoisted level's core set (anchor hanchor[j])
+    // or the last vertex's fixed set F (anchor fanchor), built once per anchor
+    // node.  A base anchored at a holds the set under the conditions on
+    // phi(0..a); the vertices phi(a+1..s) it may still hold are removed from
+    // the counts below.  Other sets are built per node.  One call site of
+    // collect for all of them (the kernel's code stays small).
+#pragma unroll 1
+    for (int u = 0; u < t; ++u) {
+      const int j = s + 1 + u;
+      // 0: built per node; 1: the last vertex's F; 2: a hoisted level's core
+      const int kind = (LAB && j == k - 1) ? 1 : (LAB && j < k - 1 && W.hanchor[j] >= 0) ? 2 : 0;
+      const int anc = kind == 1 ? W.fanchor : kind == 2 ? W.hanchor[j] : s;
+      int32_t n;
+      if (kind == 1 && W.fvalid == 2) return -1;  // F does not fit
+      if ((kind == 1 && W.fvalid == 1) || (kind == 2 && W.h[j].core)) {
+        n = kind == 1 ? W.fn : W.h[j].nprod;
+      } else {
+        n = collect(j, anc, j == k - 1 ? fbuf() : buf(j));
+        if (lane == 0) {
+          if (kind == 1) {  // as build_fixed leaves it
+            W.fn = max(n, 0);
+            W.fvalid = n < 0 ? 2 : 1;
+          } else if (kind == 2 && n >= 0) {  // as build_core leaves it, without publishing any item
+            LevelHdr &H = W.h[j];
+            H.nprod = n;
+            H.core = 1;
+            H.complete = 0;
+            H.spos = H.send = 0;
+          } else if (j == k - 1) {
+            W.fvalid = 0;  // F's buffer now holds this node's set
+          } else {
+            W.h[j].complete = 0;
+          }
+        }
+        __syncwarp();
+        if (n < 0) return -1;
+      }
+      if (n == 0) return 0;  // an empty set: no leaves
+      if (lane == 0) {
+        W.tn[u] = n;
+        W.tanc[u] = (int8_t)anc;
+      }
+      __syncwarp();
+    }
+    const long long s0 = tail_size(s, t, 0), s1 = tail_size(s, t, 1);
+    const bool e01 = !LAB || P.label[s + 1] == P.label[s + 2];
+    if (t == 2) return s0 * s1 - (e01 ? tail_common(s, t, 3u) : 0);
+    const long long s2 = tail_size(s, t, 2);
+    long long c = s0 * s1 * s2;
     const bool e02 = !LAB || P.label[s + 1] == P.label[s + 3];
     const bool e12 = !LAB || P.label[s + 2] == P.label[s + 3];
-    if (e02) c -= (long long)common_count(A0, n0, A2, n2) * n1;
-    if (e12) c -= (long long)common_count(A1, n1, A2, n2) * n0;
-    if (e01 && e02) c += 2ll * common_count(A0, n0, A1, n1, A2, n2);
+    if (e01) c -= tail_common(s, t, 3u) * s2;
+    if (e02) c -= tail_common(s, t, 5u) * s1;
+    if (e12) c -= tail_common(s, t, 6u) * s0;
+    if (e01 && e02) c += 2ll * tail_common(s, t, 7u);
+    return c;
+  }
+
+  // Base set u of the tail rooted at level s (t sets): buffer and size.
+  __device__ __forceinline__ const int32_t *tail_base(int s, int t, int u) {
+    return u == t - 1 ? fbuf() : buf(s + 1 + u);
+  }
+  // Does base u hold phi(m) for this lane's m (m <= s)?  Such a value is not
+  // in the node's set when m lies after the base's anchor.
+  __device__ __forceinline__ bool tail_holds(int s, int t, int u) {
+    if (!LAB || lane > s) return false;  // unlabeled bases are built per node
+    const int32_t *B = tail_base(s, t, u);
+    const int32_t nb = W.tn[u], x = W.phi[lane];
+    const int32_t q = lower_bound(B, 0, nb, x);
+    return q < nb && B[q] == x;
+  }
+  __device__ long long tail_size(int s, int t, int u) {
+    const bool lost = lane > W.tanc[u] && tail_holds(s, t, u);
+    return (long long)W.tn[u] - __popc(__ballot_sync(kFull, lost));
+  }
+  // |intersection of the node's sets in `mask`| (bits of u; two or three sets)
+  __device__ long long tail_common(int s, int t, unsigned mask) {
+    const int u = __ffs(mask) - 1, v = __ffs(mask & (mask - 1)) - 1;
+    const int w = mask == 7u ? 2 : -1;
+    long long c = common_count(tail_base(s, t, u), W.tn[u], tail_base(s, t, v), W.tn[v],
+                               w >= 0 ? tail_base(s, t, w) : nullptr, w >= 0 ? W.tn[w] : 0);
+    if (LAB) {
+      int after = max((int)W.tanc[u], (int)W.tanc[v]);
+      if (w >= 0) after = max(after, (int)W.tanc[w]);
+      const bool lost = lane > after && tail_holds(s, t, u) && tail_holds(s, t, v) && (w < 0 || tail_holds(s, t, w));
+      c -= __popc(__ballot_sync(kFull, lost));
+    }
     return c;
   }
 

@@ -123,13 +123,16 @@ def test_powerlaw_labeled_random(cl):
         cl.check(random_pattern(4 + t % 4, 0.45, 4, rng), True)
 
 
-@pytest.mark.parametrize("opt", [{}, {"chunk_cap": 64}, {"tail_count": -1}, {"dead_prune": -1}])
+@pytest.mark.parametrize("opt", [{}, {"chunk_cap": 64}, {"tail_count": -1}, {"dead_prune": -1},
+                                 {"level_hoist": -1}])
 def test_independent_tails(er, cl_small, T, opt):
     """Patterns whose last two or three vertices hang only on earlier ones and
     not on each other: a node at the root of that tail counts its leaves by
-    inclusion-exclusion over their candidate sets.  With 64-entry buffers the
-    power-law graph's hub sets do not fit and those nodes descend the
-    ordinary way; tail_count=-1 enumerates everywhere."""
+    inclusion-exclusion over their candidate sets, on labeled plans taken from
+    hoisted levels' core sets and the last vertex's fixed set where those are
+    anchored earlier (level_hoist=-1: every set built per node).  With 64-entry
+    buffers the power-law graph's hub sets do not fit and those nodes descend
+    the ordinary way; tail_count=-1 enumerates everywhere."""
     for i in range(8):  # the config-3 patterns: five of them have such a tail
         er.check(T.gen_pattern(6 + i % 2, 0.4, 4, 3000 + i), True, **opt)
     rng = random.Random(12)
