@@ -137,7 +137,7 @@ int tdfs_plan_free(tdfs_plan *p);
 int tdfs_count(tdfs_graph *g, const tdfs_plan *p, const tdfs_options *opt, uint64_t *count,
                float *kernel_ms);
 
-/* ---- batched launch (no reference counterpart; the north-star batching) --
+/* ---- batched launch (no reference counterpart) ----------------------------
  * All plans run in one persistent launch; counts[i] belongs to plans[i]. */
 int tdfs_count_batch(tdfs_graph *g, const tdfs_plan *const *plans, int nplans,
                      const tdfs_options *opt, uint64_t *counts, float *kernel_ms);
@@ -181,7 +181,7 @@ int tdfs_selftest_wait_limit(tdfs_graph *g, int wait_limit_ms, float *kernel_ms)
 int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, const tdfs_options *base,
                   int sample_stride, tdfs_options *best, float *best_ms);
 
-/* ---- serving (no reference counterpart; the north-star served stream) -----
+/* ---- serving (no reference counterpart) -----------------------------------
  * A continuous-batching server over one device-resident graph: queries
  * submitted at any time are admitted into a running persistent kernel as
  * in-flight places and device memory free up, so their work overlaps on the
