@@ -40,3 +40,27 @@ def test_no_gpu_fails_loudly(T):
         assert e.code == 4 and "no CUDA device" in str(e)
     else:
         raise AssertionError("graph upload must fail without a GPU")
+
+
+def test_options_layout_matches_header(T, tmp_path):
+    """The ctypes mirror of tdfs_options has the header's fields, in order, at
+    the offsets a C compiler gives them (checked with gcc on the header)."""
+    import ctypes
+    import re
+    import subprocess
+    hdr = os.path.join(os.path.dirname(__file__), "..", "include", "tdfs.h")
+    text = open(hdr).read()
+    body = text[text.index("typedef struct {", text.index("Launch knobs")):text.index("} tdfs_options;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    fields = re.findall(r"\b(\w+)\s*;", body)
+    assert [f for f, _ in T.Options._fields_] == fields
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "tdfs.h"\nint main(void) {\n'
+                   '  printf("%zu\\n", sizeof(tdfs_options));\n' +
+                   "".join(f'  printf("%zu\\n", offsetof(tdfs_options, {f}));\n' for f in fields) +
+                   "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.dirname(hdr), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(T.Options)
+    assert got[1:] == [getattr(T.Options, f).offset for f in fields]
