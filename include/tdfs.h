@@ -41,7 +41,8 @@ typedef struct tdfs_csr tdfs_csr;     /* host CSR (generators, file reader) */
 typedef struct {
   int warps_per_block;  /* warps per CTA */
   int blocks_per_sm;    /* resident CTAs per SM */
-  int chunk_cap;        /* candidate slots per DFS level (multiple of 32) */
+  int chunk_cap;        /* candidate slots per DFS level (multiple of 32; 0 auto: 128 for patterns
+                           of at most 4 vertices, 512 for 5, 256 for 6 and 7, per launch) */
   int steal;            /* 1: intra-block work stealing + global split queue; 0: off; -1 auto */
   int merge_window;     /* merge-window size in ints (0 auto, -1 = binary search only) */
   int64_t edge_begin;   /* level-0 directed-edge range [edge_begin, edge_end) */

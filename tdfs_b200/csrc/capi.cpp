@@ -61,7 +61,10 @@ int launch_shape(const tdfs_graph *g, int kmax, bool labeled, const tdfs_options
   std::memset(&s, 0, sizeof s);
   s.warps_per_block = o.warps_per_block > 0 ? o.warps_per_block : 8;
   if (s.warps_per_block > 8) return fail(TDFS_ERR_ARG, "warps_per_block must be <= 8");
-  int cap = o.chunk_cap > 0 ? o.chunk_cap : (kmax >= 6 ? 256 : 512);
+  // automatic depth per launch: small for patterns of at most 4 vertices
+  // (their short DFS gains from more resident warps), large for 5, and 256
+  // for the two extra stored levels of 6 and 7
+  int cap = o.chunk_cap > 0 ? o.chunk_cap : (kmax >= 6 ? 256 : kmax == 5 ? 512 : 128);
   cap = (cap + 31) & ~31;
   if (cap < 64 || cap > 8192) return fail(TDFS_ERR_ARG, "chunk_cap must lie in [64, 8192]");
   int window = o.merge_window == 0 ? 128 : (o.merge_window < 0 ? 0 : o.merge_window);
@@ -523,10 +526,11 @@ int tdfs_autotune(tdfs_graph *g, const tdfs_plan *const *plans, int nplans, cons
   if (sample_stride < 1) sample_stride = 1;
   // resolve the automatic values so every knob has a concrete start
   tdfs_options cur = b;
-  int kmax = 3;
-  for (int i = 0; i < nplans; ++i) kmax = std::max(kmax, plans[i]->host.k);
   if (cur.warps_per_block <= 0) cur.warps_per_block = 8;
-  if (cur.chunk_cap <= 0) cur.chunk_cap = kmax >= 6 ? 256 : 512;
+  // chunk_cap stays automatic (0) unless a fixed depth wins: the automatic
+  // depth is chosen per launch, so a batch that mixes modes gets each
+  // launch's own
+  cur.chunk_cap = std::max(0, cur.chunk_cap);
   if (cur.merge_window == 0) cur.merge_window = 128;
   if (cur.steal < 0) cur.steal = 1;
   if (cur.steal_min <= 0) cur.steal_min = 2;
